@@ -1,0 +1,244 @@
+/*
+ * cosims_cuda.h -- C ABI of the B200 trajectory-method CCS engine.
+ *
+ * The reference (CoSIMS) has no plugin or operator API: its seam is the
+ * in-process loop body of monteTraj::runTraj, which samples a start state
+ * (monteTraj::setUpTraj, monteTraj.cpp:174-278), integrates it
+ * (diffEqSolver::verletVel, diffEqSolver.cpp:81-211, forces from
+ * forceAccel::getReducedVec / getPotential, forceAccel.cpp:887-982) and
+ * accumulates pi*b_max^2*P*(1-cos chi) (monteTraj::runThreads,
+ * monteTraj.cpp:456-502).  One call of this ABI replaces that whole OpenMP
+ * loop (monteTraj.cpp:352-369) for a batch of trajectories.
+ *
+ * Conventions
+ *   - Plain C types only; no C++ or CUDA types cross the boundary.  Streams are
+ *     passed as `void*` (a cudaStream_t, NULL = the legacy default stream).
+ *   - Every entry point returns a cosims_status; cosims_last_error() returns a
+ *     thread-local message for the last failure on the calling thread.
+ *   - The caller owns every host array.  A context copies the molecule to the
+ *     device at creation and owns that copy, its scratch buffers and graphs.
+ *   - A context is re-entrant per stream: calls on one context must be
+ *     serialised by the caller (one host thread per context, or a lock).
+ *   - Units are the reference's: Angstrom, picosecond, unified atomic mass
+ *     unit, Kelvin, elementary charge (molecule2.h:69-72, maxBoltz.h:29).
+ */
+#ifndef COSIMS_CUDA_H
+#define COSIMS_CUDA_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define COSIMS_ABI_VERSION 1
+
+typedef enum cosims_status {
+    COSIMS_OK = 0,
+    COSIMS_ERR_INVALID = 1,     /* bad argument or inconsistent molecule/params */
+    COSIMS_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    COSIMS_ERR_NOMEM = 3,       /* device or host allocation failed */
+    COSIMS_ERR_IO = 4,          /* file could not be read or parsed */
+    COSIMS_ERR_TIMEOUT = 5,     /* a bounded device wait gave up */
+    COSIMS_ERR_UNSUPPORTED = 6, /* no sm_100 device, or a size beyond a limit */
+    COSIMS_ERR_BUSY = 7         /* serving queue full */
+} cosims_status;
+
+/* Force variants, numbered as forceAccel::setClusters selects them
+ * (forceAccel.cpp:125-140). */
+typedef enum cosims_force_type {
+    COSIMS_FORCE_MULTIPOLE_CUTOFF = 1,   /* multipoleCutoff   forceAccel.cpp:221-445 */
+    COSIMS_FORCE_MULTIPOLE_ONLY = 2,     /* multipoleOnly     forceAccel.cpp:447-633 */
+    COSIMS_FORCE_DISPERSION_ONLY = 3,    /* dispersionOnly    forceAccel.cpp:635-749 */
+    COSIMS_FORCE_CHARGE_DIPOLE_LJ = 4,   /* chargeDipoleLJ    forceAccel.cpp:751-805 */
+    COSIMS_FORCE_DISPERSION_NOCHARGE = 5,/* dispersionNoCharge forceAccel.cpp:807-854 */
+    COSIMS_FORCE_DISPERSION_FULL = 6     /* dispersionFull    forceAccel.cpp:856-884 */
+} cosims_force_type;
+
+typedef enum cosims_precision {
+    /* The reference method in FP64, one thread per trajectory, the
+     * reference's operation order (bit-for-bit the same force sums). */
+    COSIMS_PRECISION_PLAIN_F64 = 0,
+    /* Pair forces in FP32 on molecule-centred coordinates; positions,
+     * velocities, the energy check, 1-cos(chi) and the CCS sums in FP64. */
+    COSIMS_PRECISION_MIXED = 1
+} cosims_precision;
+
+/* One molecule after the reference's setup: COM-centred and rotated into its
+ * inertia frame (molecule2::setInertia, molecule2.cpp:1131-1308), with the
+ * force-field terms of molecule2::setMolProperties (molecule2.cpp:770-903)
+ * and the PCM clusters of forceAccel::setClusters (forceAccel.cpp:53-141).
+ * All arrays are host memory, file order unless stated. */
+typedef struct cosims_molecule {
+    int32_t n_atoms;
+    const double *x, *y, *z;      /* coordinates, Angstrom                     */
+    const double *charge;         /* partial charges, e                         */
+    const double *sig6;           /* sigma^6 (dataList::sigAvg6)                */
+    const double *eps24m;         /* 24 eps'/mu (dataList::eps24_mass; atom 0 is
+                                     not divided by mu, molecule2.cpp:862-863)  */
+    const double *eps4;           /* 4 eps' (dataList::eps4)                    */
+    /* PCM clusters; n_clusters = 0 when neither cut-off scheme is on. */
+    int32_t n_clusters;
+    const int32_t *cluster_offset;   /* n_clusters + 1 prefix offsets           */
+    const int32_t *cluster_atoms;    /* member atom indices, reference order    */
+    const double *cluster_pos;       /* 3 * n_clusters: centre used by forces   */
+    const double *cluster_radius;    /* max member distance from the centre     */
+    const double *cluster_charge;    /* total charge                            */
+    const double *cluster_dipole;    /* 3 * n_clusters                          */
+    const double *cluster_quad;      /* 9 * n_clusters, row-major               */
+    const int32_t *cluster_replaced; /* centre replaced by centre of charge     */
+} cosims_molecule;
+
+/* Scalars of the trajectory path, as the reference computes them in
+ * monteTraj::monteTraj (monteTraj.cpp:26-142) and fileParams defaults. */
+typedef struct cosims_params {
+    int32_t force_type;       /* cosims_force_type                              */
+    int32_t multipole_order;  /* multipole_order_ext (0, 1 or 2)                */
+    int32_t projection;       /* projection_ext: ellipsoid start/stop surface   */
+    int32_t charged;          /* charge_ext: induced-dipole energy term on      */
+    double dt;                /* dt_ext, ps                                      */
+    double mu;                /* mass_ext: He-molecule reduced mass, u          */
+    double dipole_scalar;     /* 28276.01363 / mu (forceAccel.cpp:35)           */
+    double r_disp;            /* dispersion_radius_ext                          */
+    double r_mp;              /* multipole_radius_ext                           */
+    double ell_a, ell_b, ell_c; /* enlarged ellipsoid axes (impactParam a,b,c)  */
+    double b_max;             /* impactParam::getMax()                          */
+    double start_dist;        /* float(b_max): monteTraj::maxDist is a float    */
+    double g_min, g_max;      /* velocity window (monteTraj.cpp:54-55)          */
+    double vdist_a;           /* beta / 2 = mu / (2 k T)                        */
+    double vdist_norm;        /* renormalised g^5 exp(-a g^2) normalisation     */
+    double vdist_max;         /* density at the mode (maxVelDistr)              */
+    double ccs_const;         /* const1 * const2 (monteTraj.cpp:91-94, :472)    */
+    int64_t max_steps;        /* hard cap on integration steps per trajectory;
+                                 the reference has none (0 = default 2^22)      */
+} cosims_params;
+
+/* Per-trajectory status bits. */
+#define COSIMS_TRAJ_HIT       0x1u  /* start state reached the ellipsoid        */
+#define COSIMS_TRAJ_SUCCESS   0x2u  /* verletVel returned true                  */
+#define COSIMS_TRAJ_STEPCAP   0x4u  /* stopped by max_steps (counted as failed) */
+#define COSIMS_TRAJ_ETRIES_SHIFT 8  /* bits 8..15: energy-check retries         */
+#define COSIMS_TRAJ_OTRIES_SHIFT 16 /* bits 16..23: orbit-detector dt shrinks   */
+
+/* One trajectory's result.  chi follows the reference's conventions: the
+ * scattering angle on success, pi/2 on failure (diffEqSolver.cpp:208), 0 on
+ * an ellipsoid miss (monteTraj.cpp:366-367). */
+typedef struct cosims_traj_out {
+    double chi;
+    double de_pct;   /* energy deviation in % at the accepted exit, else 0      */
+    int32_t steps;   /* localThreadParams::stepCount as the reference sets it   */
+    uint32_t status; /* COSIMS_TRAJ_* bits                                      */
+} cosims_traj_out;
+
+/* Sampled start values of one trajectory (monteTraj.cpp:203-253). */
+typedef struct cosims_traj_in {
+    double b, phi, theta, gamma, g;
+} cosims_traj_in;
+
+/* Sums of one CCS integral, reduced in a fixed order (deterministic). */
+typedef struct cosims_ccs_sums {
+    double sum;           /* sum of ccs_const * (1 - cos|chi|)                   */
+    double sum2;          /* sum of squares                                      */
+    double max_de_pct;    /* max energy deviation over successes                 */
+    int64_t n;            /* trajectories processed (misses included)            */
+    int64_t n_hit;        /* start states that reached the ellipsoid             */
+    int64_t n_success;    /* verletVel successes                                 */
+    int64_t n_eff;        /* the reference's success count for Omega = sum/n_eff:
+                             n minus the failures its one-thread bookkeeping
+                             still holds at the end (monteTraj.cpp:380-381,
+                             504-521); see cosims_run_sampled                   */
+    int64_t steps;        /* integration steps, all attempts                     */
+    int64_t pair_evals;   /* atom-pair interactions evaluated (roofline work)    */
+} cosims_ccs_sums;
+
+typedef struct cosims_ctx cosims_ctx;
+
+/* ---- library ------------------------------------------------------------ */
+int32_t cosims_abi_version(void);
+const char *cosims_last_error(void);
+/* Number of usable CUDA devices (0 when none).  Never initialises a context. */
+int32_t cosims_device_count(void);
+
+/* ---- one molecule on the device ---------------------------------------- */
+/* Copies mol and par to `device` and prepares the shared-memory image.
+ * precision: cosims_precision.  Replaces monteTraj's per-molecule state
+ * (gasAtom.setMol -> forceAccel::setMol/setClusters, monteTraj.cpp:88). */
+cosims_status cosims_ctx_create(const cosims_molecule *mol, const cosims_params *par,
+                                int32_t precision, int32_t device, cosims_ctx **out);
+void cosims_ctx_destroy(cosims_ctx *ctx);
+
+/* Launch shape: lanes per trajectory (1,2,4,...,32; the plain form accepts 1
+ * only) and threads per CTA.  0 keeps the current choice. */
+cosims_status cosims_ctx_set_launch(cosims_ctx *ctx, int32_t group_lanes,
+                                    int32_t block_threads);
+cosims_status cosims_ctx_get_launch(const cosims_ctx *ctx, int32_t *group_lanes,
+                                    int32_t *block_threads);
+
+/* Fixed-list form: integrate n given start states (pos0, vel0: 3n doubles each,
+ * host memory) and write n results to out (host).  Replaces, per trajectory,
+ * diffEqSolver::verletVel (diffEqSolver.cpp:81-211) as monteTraj.cpp:362-364
+ * calls it.  Blocks until the results are on the host. */
+cosims_status cosims_run_list(cosims_ctx *ctx, const double *pos0, const double *vel0,
+                              int64_t n, cosims_traj_out *out, void *stream);
+/* Same with device pointers; stream-ordered, returns without synchronising. */
+cosims_status cosims_run_list_device(cosims_ctx *ctx, const double *d_pos0,
+                                     const double *d_vel0, int64_t n,
+                                     cosims_traj_out *d_out, void *stream);
+
+/* Sampled form: trajectories first_index .. first_index+n-1 of the stream
+ * keyed by seed.  Start values come from counter-based Philox4x32-10 on the
+ * device (one counter block per trajectory and attempt), with the
+ * reference's distributions (monteTraj.cpp:203-253): g ~ g^5 exp(-a g^2) on
+ * [g_min, g_max], theta ~ sin(theta), b ~ b on [0, b_max], phi and gamma
+ * uniform.  Replaces one CCS integral of monteTraj::runTraj
+ * (monteTraj.cpp:301-388).  update_every is the reference's progress
+ * interval ceil(print_rate / threads) (monteTraj.cpp:340); n_eff reproduces
+ * its one-thread success count.  sums: host; inputs/outs: optional host
+ * arrays of n entries (NULL to skip).  Blocks until done. */
+cosims_status cosims_run_sampled(cosims_ctx *ctx, uint64_t seed, int64_t first_index,
+                                 int64_t n, int64_t update_every, cosims_ccs_sums *sums,
+                                 cosims_traj_in *inputs, cosims_traj_out *outs,
+                                 void *stream);
+/* Same with a device-resident sums record; stream-ordered, no host sync. */
+cosims_status cosims_run_sampled_device(cosims_ctx *ctx, uint64_t seed,
+                                        int64_t first_index, int64_t n,
+                                        int64_t update_every,
+                                        cosims_ccs_sums *d_sums, void *stream);
+/* Start states only: the sampler and the ellipsoid projection
+ * (monteTraj.cpp:235-277) for trajectories first_index..first_index+n-1.
+ * Host outputs; pos0/vel0 are 3n doubles; hit is n int32. */
+cosims_status cosims_sample_inputs(cosims_ctx *ctx, uint64_t seed, int64_t first_index,
+                                   int64_t n, cosims_traj_in *inputs, double *pos0,
+                                   double *vel0, int32_t *hit, void *stream);
+
+/* ---- batched: many molecules, one persistent launch -------------------- */
+typedef struct cosims_batch cosims_batch;
+
+/* mols/pars: n_mol entries.  Molecules are packed into one device arena and
+ * staged per CTA with bulk copies when a work item switches molecule. */
+cosims_status cosims_batch_create(const cosims_molecule *mols, const cosims_params *pars,
+                                  int32_t n_mol, int32_t precision, int32_t device,
+                                  cosims_batch **out);
+void cosims_batch_destroy(cosims_batch *b);
+/* Picks lanes-per-trajectory per molecule and the work-item size by timing
+ * short trial launches (results cached by atom count and force type). */
+cosims_status cosims_batch_autotune(cosims_batch *b, void *stream);
+/* Runs n_traj[i] sampled trajectories of molecule i (seed[i], first_index[i])
+ * through one persistent kernel fed by a device work queue; the launch is
+ * captured in a CUDA graph on first use and replayed.  sums: n_mol records
+ * (host).  Blocks until done. */
+cosims_status cosims_batch_run(cosims_batch *b, const uint64_t *seed,
+                               const int64_t *first_index, const int64_t *n_traj,
+                               cosims_ccs_sums *sums, void *stream);
+/* Device-resident form of cosims_batch_run: seeds/first/n and sums stay on
+ * the device (host arrays are copied once at the call); no host sync. */
+cosims_status cosims_batch_run_async(cosims_batch *b, const uint64_t *seed,
+                                     const int64_t *first_index, const int64_t *n_traj,
+                                     cosims_ccs_sums *d_sums, void *stream);
+cosims_status cosims_batch_get_launch(const cosims_batch *b, int32_t mol,
+                                      int32_t *group_lanes, int32_t *item_traj);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* COSIMS_CUDA_H */
