@@ -67,7 +67,9 @@ class TrajIn(C.Structure):
 class CcsSums(C.Structure):
     _fields_ = [("sum", C.c_double), ("sum2", C.c_double), ("max_de_pct", C.c_double),
                 ("n", C.c_int64), ("n_hit", C.c_int64), ("n_success", C.c_int64),
-                ("n_eff", C.c_int64), ("steps", C.c_int64), ("pair_evals", C.c_int64)]
+                ("n_eff", C.c_int64), ("steps", C.c_int64), ("force_evals", C.c_int64),
+                ("pot_evals", C.c_int64), ("pair_lj", C.c_int64), ("pair_es", C.c_int64),
+                ("pair_pot", C.c_int64), ("far_terms", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

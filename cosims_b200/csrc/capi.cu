@@ -1,0 +1,531 @@
+// capi.cu -- the C ABI (include/cosims_cuda.h): contexts, device images,
+// launch sizing and the list / sampled run paths.
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "capi_internal.h"
+
+namespace cosims {
+
+static thread_local std::string g_last_error;
+
+cosims_status fail(cosims_status s, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return s;
+}
+
+cosims_status cuda_fail(cudaError_t e, const char *what) {
+  return fail(COSIMS_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+const char *last_error() { return g_last_error.c_str(); }
+
+// ---- image building ----------------------------------------------------------
+
+namespace {
+
+struct Builder {
+  std::vector<unsigned char> buf;
+  uint32_t add(const void *src, size_t bytes) {
+    size_t off = (buf.size() + 15) & ~size_t(15);
+    buf.resize(off + bytes);
+    if (bytes) std::memcpy(buf.data() + off, src, bytes);
+    return (uint32_t)off;
+  }
+  void finish() { buf.resize((buf.size() + 15) & ~size_t(15)); }
+};
+
+}  // namespace
+
+cosims_status validate(const cosims_molecule *mol, const cosims_params *par) {
+  if (!mol || !par) return fail(COSIMS_ERR_INVALID, "molecule and params are required");
+  if (mol->n_atoms <= 0 || mol->n_atoms > kMaxAtoms)
+    return fail(COSIMS_ERR_UNSUPPORTED, "n_atoms %d outside 1..%d", mol->n_atoms, kMaxAtoms);
+  if (!mol->x || !mol->y || !mol->z || !mol->charge || !mol->sig6 || !mol->eps24m || !mol->eps4)
+    return fail(COSIMS_ERR_INVALID, "molecule arrays must not be NULL");
+  if (par->force_type < 1 || par->force_type > 6)
+    return fail(COSIMS_ERR_INVALID, "force_type %d outside 1..6", par->force_type);
+  const bool uses = par->force_type != 4 && par->force_type != 6;
+  if (mol->n_clusters < 0 || mol->n_clusters > kMaxClusters)
+    return fail(COSIMS_ERR_UNSUPPORTED, "n_clusters %d outside 0..%d", mol->n_clusters,
+                kMaxClusters);
+  if (uses) {
+    if (mol->n_clusters == 0)
+      return fail(COSIMS_ERR_INVALID, "force_type %d needs clusters", par->force_type);
+    if (!mol->cluster_offset || !mol->cluster_atoms || !mol->cluster_pos ||
+        !mol->cluster_radius || !mol->cluster_charge || !mol->cluster_dipole ||
+        !mol->cluster_quad || !mol->cluster_replaced)
+      return fail(COSIMS_ERR_INVALID, "cluster arrays must not be NULL");
+    if (mol->cluster_offset[0] != 0 || mol->cluster_offset[mol->n_clusters] != mol->n_atoms)
+      return fail(COSIMS_ERR_INVALID, "cluster offsets must run from 0 to n_atoms");
+    std::vector<char> seen(mol->n_atoms, 0);
+    for (int c = 0; c < mol->n_clusters; c++) {
+      if (mol->cluster_offset[c + 1] < mol->cluster_offset[c])
+        return fail(COSIMS_ERR_INVALID, "cluster offsets must not decrease");
+      for (int k = mol->cluster_offset[c]; k < mol->cluster_offset[c + 1]; k++) {
+        int a = mol->cluster_atoms[k];
+        if (a < 0 || a >= mol->n_atoms || seen[a])
+          return fail(COSIMS_ERR_INVALID, "clusters must partition the atoms");
+        seen[a] = 1;
+      }
+    }
+  }
+  if (!(par->dt > 0) || !(par->mu > 0) || !(par->ell_a > 0) || !(par->ell_b > 0) ||
+      !(par->ell_c > 0))
+    return fail(COSIMS_ERR_INVALID, "dt, mu and the ellipsoid axes must be positive");
+  if (par->multipole_order < 0 || par->multipole_order > 2)
+    return fail(COSIMS_ERR_INVALID, "multipole_order must be 0, 1 or 2");
+  return COSIMS_OK;
+}
+
+DevParams make_dev_params(const cosims_params *p) {
+  DevParams d;
+  d.force_type = p->force_type;
+  d.multipole_order = p->multipole_order;
+  d.projection = p->projection;
+  d.charged = p->charged;
+  d.dt = p->dt; d.mu = p->mu; d.dipole_scalar = p->dipole_scalar;
+  d.r_disp = p->r_disp; d.r_mp = p->r_mp;
+  d.ell_a = p->ell_a; d.ell_b = p->ell_b; d.ell_c = p->ell_c;
+  d.max_rad = std::max(p->ell_a, std::max(p->ell_b, p->ell_c));   // diffEqSolver.cpp:99
+  d.b_max = p->b_max; d.start_dist = p->start_dist;
+  d.g_min = p->g_min; d.g_max = p->g_max;
+  d.vdist_a = p->vdist_a; d.vdist_norm = p->vdist_norm; d.vdist_max = p->vdist_max;
+  d.ccs_const = p->ccs_const;
+  d.max_steps = p->max_steps;
+  return d;
+}
+
+void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h64,
+                  HostImage &h32) {
+  const int n = m->n_atoms;
+  const bool uses = p->force_type != 4 && p->force_type != 6;
+  const int nc = uses ? m->n_clusters : 0;
+  std::vector<int> order(n), perm(n), cid(n, 0), coff(nc + 1, 0);
+  if (uses) {
+    for (int c = 0; c < nc; c++) {
+      coff[c + 1] = m->cluster_offset[c + 1];
+      for (int k = m->cluster_offset[c]; k < m->cluster_offset[c + 1]; k++) {
+        order[k] = m->cluster_atoms[k];
+        cid[k] = c;
+      }
+    }
+  } else {
+    for (int i = 0; i < n; i++) order[i] = i;
+  }
+  for (int k = 0; k < n; k++) perm[order[k]] = k;
+
+  std::vector<AtomF64> a64(n);
+  std::vector<AtomF32> a32(n);
+  for (int k = 0; k < n; k++) {
+    const int i = order[k];
+    AtomF64 &A = a64[k];
+    A.x = m->x[i]; A.y = m->y[i]; A.z = m->z[i]; A.q = m->charge[i];
+    A.sig6 = m->sig6[i]; A.eps24m = m->eps24m[i]; A.eps4 = m->eps4[i];
+    AtomF32 &F = a32[k];
+    F.x = (float)A.x; F.y = (float)A.y; F.z = (float)A.z; F.q = (float)A.q;
+    F.sig6 = (float)A.sig6; F.eps24m = (float)A.eps24m;
+    F.cid = (uint32_t)cid[k]; F.pad = 0.f;
+  }
+  std::vector<ClusterF64> c64(nc);
+  std::vector<ClusterF32> c32(nc);
+  for (int c = 0; c < nc; c++) {
+    ClusterF64 &C = c64[c];
+    std::memset(&C, 0, sizeof C);
+    C.cx = m->cluster_pos[3 * c]; C.cy = m->cluster_pos[3 * c + 1];
+    C.cz = m->cluster_pos[3 * c + 2];
+    double a = p->r_mp + m->cluster_radius[c];      // forceAccel.cpp:253-256
+    a *= a;
+    double b = p->r_disp + m->cluster_radius[c];
+    b *= b;
+    C.mpr2 = a; C.dr2 = b;
+    C.q = m->cluster_charge[c];
+    for (int k = 0; k < 3; k++) C.dip[k] = m->cluster_dipole[3 * c + k];
+    for (int k = 0; k < 9; k++) C.quad[k] = m->cluster_quad[9 * c + k];
+    // multipoleCutoff's far band reads atom index n = the cluster index
+    C.qsig6 = c < n ? m->sig6[c] : 0.0;
+    C.qeps = c < n ? m->eps24m[c] : 0.0;
+    C.a0 = coff[c]; C.a1 = coff[c + 1];
+    C.replaced = m->cluster_replaced[c];
+    ClusterF32 &F = c32[c];
+    std::memset(&F, 0, sizeof F);
+    F.cx = C.cx; F.cy = C.cy; F.cz = C.cz; F.mpr2 = C.mpr2; F.dr2 = C.dr2;
+    F.q = (float)C.q;
+    for (int k = 0; k < 3; k++) F.dip[k] = (float)C.dip[k];
+    for (int k = 0; k < 9; k++) F.quad[k] = (float)C.quad[k];
+    F.qsig6 = (float)C.qsig6; F.qeps = (float)C.qeps;
+    F.replaced = C.replaced; F.a0 = C.a0; F.a1 = C.a1;
+  }
+
+  Builder b64;
+  MolImage &i64 = h64.img;
+  std::memset(&i64, 0, sizeof i64);
+  i64.off[S_ATOMS] = b64.add(a64.data(), sizeof(AtomF64) * n);
+  i64.off[S_PERM] = b64.add(perm.data(), 4 * n);
+  i64.off[S_CLUSTERS] = b64.add(c64.data(), sizeof(ClusterF64) * nc);
+  b64.finish();
+  i64.bytes = (uint32_t)b64.buf.size();
+  i64.n_atoms = n;
+  i64.n_clusters = nc;
+  i64.uses_clusters = uses ? 1 : 0;
+  h64.bytes = std::move(b64.buf);
+
+  Builder b32;
+  MolImage &i32 = h32.img;
+  std::memset(&i32, 0, sizeof i32);
+  i32.off[S_ATOMS] = b32.add(a32.data(), sizeof(AtomF32) * n);
+  i32.off[S_CLUSTERS] = b32.add(c32.data(), sizeof(ClusterF32) * nc);
+  b32.finish();
+  i32.bytes = (uint32_t)b32.buf.size();
+  i32.n_atoms = n;
+  i32.n_clusters = nc;
+  i32.uses_clusters = uses ? 1 : 0;
+  h32.bytes = std::move(b32.buf);
+}
+
+// ---- device helpers ------------------------------------------------------------
+
+cosims_status check_device(int device, int *sm_count, int *max_smem) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0)
+    return fail(COSIMS_ERR_UNSUPPORTED, "no CUDA device: %s", cudaGetErrorString(e));
+  if (device < 0 || device >= count)
+    return fail(COSIMS_ERR_INVALID, "device %d outside 0..%d", device, count - 1);
+  cudaDeviceProp prop;
+  e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
+  if (prop.major != 10)
+    return fail(COSIMS_ERR_UNSUPPORTED, "device %d is sm_%d%d; this build targets sm_100a",
+                device, prop.major, prop.minor);
+  *sm_count = prop.multiProcessorCount;
+  *max_smem = (int)prop.sharedMemPerBlockOptin;
+  return COSIMS_OK;
+}
+
+DeviceGuard::DeviceGuard(int dev) {
+  cudaGetDevice(&prev);
+  if (prev != dev) cudaSetDevice(dev);
+}
+DeviceGuard::~DeviceGuard() { cudaSetDevice(prev); }
+
+template <typename T>
+static cosims_status grow(T **p, int64_t *cap, int64_t need) {
+  if (*cap >= need) return COSIMS_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  int64_t n = std::max<int64_t>(need, 1024);
+  cudaError_t e = cudaMalloc((void **)p, sizeof(T) * (size_t)n);
+  if (e != cudaSuccess) return fail(COSIMS_ERR_NOMEM, "cudaMalloc of %lld bytes: %s",
+                                    (long long)(sizeof(T) * n), cudaGetErrorString(e));
+  *cap = n;
+  return COSIMS_OK;
+}
+
+// Launch shape for a context: threads per CTA, CTAs, dynamic shared memory,
+// whether the image is staged, and the per-group mode scratch.
+cosims_status launch_shape(const cosims_ctx *c, int64_t n, LaunchShape &ls) {
+  const int G = c->precision == COSIMS_PRECISION_PLAIN_F64 ? 1 : c->group_lanes;
+  int block = c->block_threads;
+  const MolImage &img = c->precision == COSIMS_PRECISION_PLAIN_F64 ? c->img64 : c->img32;
+  const int budget = c->max_smem - 1024;
+  ls.use_smem = (int)img.bytes <= budget ? 1 : 0;
+  ls.mode_stride = 0;
+  if (c->precision == COSIMS_PRECISION_MIXED && img.uses_clusters) {
+    int s = (img.n_clusters + 3) & ~3;
+    if (((s / 4) & 1) == 0) s += 4;     // odd word count: groups hit distinct banks
+    ls.mode_stride = s;
+  }
+  // shrink the CTA until image + mode scratch fit
+  for (;;) {
+    size_t smem = (ls.use_smem ? img.bytes : 0) + (size_t)(block / G) * ls.mode_stride;
+    if ((int)smem <= budget) { ls.smem = smem; break; }
+    if (ls.use_smem && block <= std::max(G, 32)) { ls.use_smem = 0; continue; }
+    if (block <= std::max(G, 32))
+      return fail(COSIMS_ERR_UNSUPPORTED, "molecule image does not fit in shared memory");
+    block /= 2;
+  }
+  ls.block = block;
+  int per_sm = 1;
+  int rc = c->precision == COSIMS_PRECISION_PLAIN_F64
+               ? plain_occupancy(block, ls.smem, &per_sm)
+               : mixed_occupancy(c->par.force_type, block, ls.smem, &per_sm);
+  if (rc != 0) return cuda_fail((cudaError_t)rc, "occupancy query");
+  per_sm = std::max(per_sm, 1);
+  const int64_t groups_needed = n;   // one group per trajectory at most
+  const int64_t groups_per_cta = block / G;
+  int64_t grid = (int64_t)per_sm * c->sm_count;
+  grid = std::min<int64_t>(grid, (groups_needed + groups_per_cta - 1) / groups_per_cta);
+  ls.grid = (int)std::max<int64_t>(grid, 1);
+  return COSIMS_OK;
+}
+
+cosims_status run_core(cosims_ctx *c, int mode, const double *d_pos0, const double *d_vel0,
+                       uint64_t seed, int64_t first, int64_t n, cosims_traj_out *d_out,
+                       cosims_traj_in *d_in, void *stream) {
+  LaunchShape ls;
+  cosims_status st = launch_shape(c, n, ls);
+  if (st != COSIMS_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemsetAsync(c->d_queue, 0, sizeof(unsigned long long), s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * C_COUNT, s);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+  if (n == 0) return COSIMS_OK;
+  TrajArgs a;
+  std::memset(&a, 0, sizeof a);
+  const bool plain = c->precision == COSIMS_PRECISION_PLAIN_F64;
+  a.img = plain ? c->img64 : c->img32;
+  a.img64 = c->img64;
+  a.par = c->par;
+  a.mode = mode;
+  a.group_lanes = plain ? 1 : c->group_lanes;
+  a.use_smem = ls.use_smem;
+  a.mode_stride = ls.mode_stride;
+  a.pos0 = d_pos0;
+  a.vel0 = d_vel0;
+  a.seed = seed;
+  a.first_index = first;
+  a.n = n;
+  a.out = d_out;
+  a.inputs = d_in;
+  a.queue = c->d_queue;
+  a.counters = c->d_counters;
+  int rc = plain ? plain_launch(a, ls.block, ls.grid, ls.smem, stream)
+                 : mixed_launch(a, ls.block, ls.grid, ls.smem, stream);
+  if (rc != 0) return cuda_fail((cudaError_t)rc, "trajectory kernel launch");
+  c->last_shape = ls;
+  return COSIMS_OK;
+}
+
+cosims_status check_error_flag(cosims_ctx *c, cudaStream_t s) {
+  unsigned long long flag = 0;
+  cudaError_t e = cudaMemcpyAsync(&flag, c->d_counters + C_ERROR, sizeof flag,
+                                  cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "trajectory run");
+  if (flag) return fail(COSIMS_ERR_TIMEOUT, "shared-memory staging wait gave up (flags %llu)", flag);
+  return COSIMS_OK;
+}
+
+}  // namespace cosims
+
+using namespace cosims;
+
+extern "C" {
+
+int32_t cosims_abi_version(void) { return COSIMS_ABI_VERSION; }
+
+const char *cosims_last_error(void) { return cosims::last_error(); }
+
+int32_t cosims_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+cosims_status cosims_ctx_create(const cosims_molecule *mol, const cosims_params *par,
+                                int32_t precision, int32_t device, cosims_ctx **out) {
+  if (!out) return fail(COSIMS_ERR_INVALID, "out is NULL");
+  *out = nullptr;
+  if (precision != COSIMS_PRECISION_PLAIN_F64 && precision != COSIMS_PRECISION_MIXED)
+    return fail(COSIMS_ERR_INVALID, "unknown precision %d", precision);
+  cosims_status st = validate(mol, par);
+  if (st != COSIMS_OK) return st;
+  int sm = 0, smem = 0;
+  st = check_device(device, &sm, &smem);
+  if (st != COSIMS_OK) return st;
+  DeviceGuard g(device);
+  cosims_ctx *c = new cosims_ctx();
+  c->device = device;
+  c->precision = precision;
+  c->sm_count = sm;
+  c->max_smem = smem;
+  c->par = make_dev_params(par);
+  c->n_atoms = mol->n_atoms;
+  build_images(mol, par, c->h64, c->h32);
+  c->img64 = c->h64.img;
+  c->img32 = c->h32.img;
+  c->group_lanes = precision == COSIMS_PRECISION_PLAIN_F64 ? 1 : default_group_lanes(mol->n_atoms);
+  c->block_threads = precision == COSIMS_PRECISION_PLAIN_F64 ? 128 : 256;
+  cudaError_t e = cudaMalloc((void **)&c->d_img64, c->img64.bytes);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_img32, c->img32.bytes);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_queue, sizeof(unsigned long long));
+  if (e == cudaSuccess)
+    e = cudaMalloc((void **)&c->d_counters, sizeof(unsigned long long) * C_COUNT);
+  if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_sums, sizeof(cosims_ccs_sums));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->d_img64, c->h64.bytes.data(), c->img64.bytes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->d_img32, c->h32.bytes.data(), c->img32.bytes, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cosims_ctx_destroy(c);
+    return fail(COSIMS_ERR_NOMEM, "context allocation: %s", cudaGetErrorString(e));
+  }
+  c->img64.gbase = c->d_img64;
+  c->img32.gbase = c->d_img32;
+  st = grow(&c->d_red, &c->red_cap, reduce_scratch_len(0));
+  if (st != COSIMS_OK) { cosims_ctx_destroy(c); return st; }
+  *out = c;
+  return COSIMS_OK;
+}
+
+void cosims_ctx_destroy(cosims_ctx *c) {
+  if (!c) return;
+  DeviceGuard g(c->device);
+  cudaFree(c->d_img64);
+  cudaFree(c->d_img32);
+  cudaFree(c->d_queue);
+  cudaFree(c->d_counters);
+  cudaFree(c->d_sums);
+  cudaFree(c->d_out);
+  cudaFree(c->d_in);
+  cudaFree(c->d_pos0);
+  cudaFree(c->d_vel0);
+  cudaFree(c->d_red);
+  cudaFree(c->d_hit);
+  delete c;
+}
+
+cosims_status cosims_ctx_set_launch(cosims_ctx *c, int32_t group_lanes, int32_t block_threads) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (group_lanes) {
+    if (group_lanes < 1 || group_lanes > 32 || (group_lanes & (group_lanes - 1)))
+      return fail(COSIMS_ERR_INVALID, "group_lanes must be a power of two in 1..32");
+    if (c->precision == COSIMS_PRECISION_PLAIN_F64 && group_lanes != 1)
+      return fail(COSIMS_ERR_INVALID, "the plain form runs one lane per trajectory");
+    c->group_lanes = group_lanes;
+  }
+  if (block_threads) {
+    if (block_threads < 32 || block_threads > 256 || (block_threads & 31))
+      return fail(COSIMS_ERR_INVALID, "block_threads must be a multiple of 32 in 32..256");
+    c->block_threads = block_threads;
+  }
+  if (c->block_threads < c->group_lanes)
+    return fail(COSIMS_ERR_INVALID, "block_threads smaller than group_lanes");
+  return COSIMS_OK;
+}
+
+cosims_status cosims_ctx_get_launch(const cosims_ctx *c, int32_t *group_lanes,
+                                    int32_t *block_threads) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (group_lanes) *group_lanes = c->precision == COSIMS_PRECISION_PLAIN_F64 ? 1 : c->group_lanes;
+  if (block_threads) *block_threads = c->block_threads;
+  return COSIMS_OK;
+}
+
+cosims_status cosims_run_list_device(cosims_ctx *c, const double *d_pos0, const double *d_vel0,
+                                     int64_t n, cosims_traj_out *d_out, void *stream) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (n < 0) return fail(COSIMS_ERR_INVALID, "n must be >= 0");
+  if (n > 0 && (!d_pos0 || !d_vel0 || !d_out))
+    return fail(COSIMS_ERR_INVALID, "pos0, vel0 and out are required");
+  DeviceGuard g(c->device);
+  return run_core(c, MODE_LIST, d_pos0, d_vel0, 0, 0, n, d_out, nullptr, stream);
+}
+
+cosims_status cosims_run_list(cosims_ctx *c, const double *pos0, const double *vel0, int64_t n,
+                              cosims_traj_out *out, void *stream) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (n < 0) return fail(COSIMS_ERR_INVALID, "n must be >= 0");
+  if (n == 0) return COSIMS_OK;
+  if (!pos0 || !vel0 || !out) return fail(COSIMS_ERR_INVALID, "pos0, vel0 and out are required");
+  DeviceGuard g(c->device);
+  cosims_status st = grow(&c->d_pos0, &c->list_cap, 3 * n);
+  if (st == COSIMS_OK) st = grow(&c->d_vel0, &c->vel_cap, 3 * n);
+  if (st == COSIMS_OK) st = grow(&c->d_out, &c->out_cap, n);
+  if (st != COSIMS_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(c->d_pos0, pos0, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->d_vel0, vel0, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return cuda_fail(e, "copy of start states");
+  st = run_core(c, MODE_LIST, c->d_pos0, c->d_vel0, 0, 0, n, c->d_out, nullptr, stream);
+  if (st != COSIMS_OK) return st;
+  e = cudaMemcpyAsync(out, c->d_out, sizeof(cosims_traj_out) * n, cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return cuda_fail(e, "copy of results");
+  return check_error_flag(c, s);
+}
+
+cosims_status cosims_run_sampled_device(cosims_ctx *c, uint64_t seed, int64_t first, int64_t n,
+                                        int64_t update_every, cosims_ccs_sums *d_sums,
+                                        void *stream) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (n < 0 || first < 0) return fail(COSIMS_ERR_INVALID, "n and first_index must be >= 0");
+  if (!d_sums) return fail(COSIMS_ERR_INVALID, "sums is NULL");
+  DeviceGuard g(c->device);
+  cosims_status st = grow(&c->d_out, &c->out_cap, n);
+  if (st != COSIMS_OK) return st;
+  st = run_core(c, MODE_SAMPLED, nullptr, nullptr, seed, first, n, c->d_out, nullptr, stream);
+  if (st != COSIMS_OK) return st;
+  int rc = reduce_launch(c->d_out, n, c->par.ccs_const,
+                         c->precision == COSIMS_PRECISION_MIXED ? 1 : 0, update_every,
+                         c->d_counters, d_sums, c->d_red, c->red_cap, stream);
+  if (rc != 0) return cuda_fail((cudaError_t)rc, "reduction launch");
+  return COSIMS_OK;
+}
+
+cosims_status cosims_run_sampled(cosims_ctx *c, uint64_t seed, int64_t first, int64_t n,
+                                 int64_t update_every, cosims_ccs_sums *sums,
+                                 cosims_traj_in *inputs, cosims_traj_out *outs, void *stream) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (!sums) return fail(COSIMS_ERR_INVALID, "sums is NULL");
+  if (n < 0 || first < 0) return fail(COSIMS_ERR_INVALID, "n and first_index must be >= 0");
+  DeviceGuard g(c->device);
+  cosims_status st = grow(&c->d_out, &c->out_cap, n);
+  if (st == COSIMS_OK && inputs) st = grow(&c->d_in, &c->in_cap, n);
+  if (st != COSIMS_OK) return st;
+  st = run_core(c, MODE_SAMPLED, nullptr, nullptr, seed, first, n, c->d_out,
+                inputs ? c->d_in : nullptr, stream);
+  if (st != COSIMS_OK) return st;
+  int rc = reduce_launch(c->d_out, n, c->par.ccs_const,
+                         c->precision == COSIMS_PRECISION_MIXED ? 1 : 0, update_every,
+                         c->d_counters, c->d_sums, c->d_red, c->red_cap, stream);
+  if (rc != 0) return cuda_fail((cudaError_t)rc, "reduction launch");
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaMemcpyAsync(sums, c->d_sums, sizeof(cosims_ccs_sums), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && outs && n)
+    e = cudaMemcpyAsync(outs, c->d_out, sizeof(cosims_traj_out) * n, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && inputs && n)
+    e = cudaMemcpyAsync(inputs, c->d_in, sizeof(cosims_traj_in) * n, cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return cuda_fail(e, "copy of results");
+  return check_error_flag(c, s);
+}
+
+cosims_status cosims_sample_inputs(cosims_ctx *c, uint64_t seed, int64_t first, int64_t n,
+                                   cosims_traj_in *inputs, double *pos0, double *vel0,
+                                   int32_t *hit, void *stream) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (n < 0 || first < 0) return fail(COSIMS_ERR_INVALID, "n and first_index must be >= 0");
+  if (n == 0) return COSIMS_OK;
+  if (!inputs || !pos0 || !vel0 || !hit)
+    return fail(COSIMS_ERR_INVALID, "inputs, pos0, vel0 and hit are required");
+  DeviceGuard g(c->device);
+  cosims_status st = grow(&c->d_in, &c->in_cap, n);
+  if (st == COSIMS_OK) st = grow(&c->d_pos0, &c->list_cap, 3 * n);
+  if (st == COSIMS_OK) st = grow(&c->d_vel0, &c->vel_cap, 3 * n);
+  if (st == COSIMS_OK) st = grow(&c->d_hit, &c->hit_cap, n);
+  if (st != COSIMS_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  int rc = sample_launch(c->par, seed, first, n, c->d_in, c->d_pos0, c->d_vel0, c->d_hit, stream);
+  if (rc != 0) return cuda_fail((cudaError_t)rc, "sampler launch");
+  cudaError_t e = cudaMemcpyAsync(inputs, c->d_in, sizeof(cosims_traj_in) * n, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(pos0, c->d_pos0, 24 * n, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(vel0, c->d_vel0, 24 * n, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(hit, c->d_hit, 4 * n, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_fail(e, "sampler");
+  return COSIMS_OK;
+}
+
+}  // extern "C"

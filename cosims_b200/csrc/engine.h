@@ -1,0 +1,140 @@
+// engine.h -- definitions shared by the host side of the C ABI and the kernels.
+//
+// Device image of one molecule.  The image is one contiguous blob in global
+// memory whose sections start on 16-byte boundaries; a CTA copies the whole
+// blob into shared memory with bulk copies (cp.async.bulk) and then reads it
+// through the same byte offsets.  Records are array-of-structs, so a kernel
+// keeps one base address per section and reaches each field by an immediate
+// offset.  Two layouts exist:
+//
+//   F64 image (plain form, and the FP64 energy check of the mixed form):
+//     AtomF64 records in "force order" -- cluster by cluster in the
+//     reference's member order for the cluster force variants (1, 2, 3, 5),
+//     file order otherwise; perm[i] = force-order slot of file atom i
+//     (getPotential walks atoms in file order); ClusterF64 records.
+//   F32 image (mixed form): AtomF32 records in force order, ClusterF32
+//     records (FP64 centre and squared radii, so the near/far tests stay FP64;
+//     FP32 multipole moments).
+#pragma once
+#include <cstdint>
+#include "cosims_cuda.h"
+
+namespace cosims {
+
+constexpr int kMaxAtoms = 16384;
+constexpr int kMaxClusters = 65535;
+constexpr int kMaxGroupLanes = 32;
+
+enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_COUNT };
+
+struct AtomF64 {            // 56 bytes
+  double x, y, z, q, sig6, eps24m, eps4;
+};
+
+struct ClusterF64 {         // 176 bytes
+  double cx, cy, cz;
+  double mpr2;              // (r_mp + R)^2    (forceAccel.cpp:253-254)
+  double dr2;               // (r_disp + R)^2  (forceAccel.cpp:255-256)
+  double q;
+  double dip[3];
+  double quad[9];           // quad[3*i+j] = quadPole[i][j]
+  double qsig6, qeps;       // sigma^6, eps24/mu of atom index n (forceAccel.cpp:353-355)
+  int32_t a0, a1;           // member range in force order
+  int32_t replaced;
+  int32_t pad;
+};
+
+struct AtomF32 {            // 32 bytes
+  float x, y, z, q;
+  float sig6, eps24m;
+  uint32_t cid;             // cluster of the atom (0 without clusters)
+  float pad;
+};
+
+struct ClusterF32 {         // 112 bytes
+  double cx, cy, cz, mpr2, dr2;
+  float q;
+  float dip[3];
+  float quad[9];
+  float qsig6, qeps;
+  int32_t replaced;
+  int32_t a0, a1;
+};
+
+static_assert(sizeof(AtomF64) == 56, "AtomF64 layout");
+static_assert(sizeof(ClusterF64) == 176, "ClusterF64 layout");
+static_assert(sizeof(AtomF32) == 32, "AtomF32 layout");
+static_assert(sizeof(ClusterF32) == 112, "ClusterF32 layout");
+
+struct MolImage {
+  const unsigned char *gbase;   // image in global memory
+  uint32_t bytes;               // image size, multiple of 16
+  int32_t n_atoms;
+  int32_t n_clusters;
+  int32_t uses_clusters;        // force variant walks clusters (1, 2, 3, 5)
+  uint32_t off[S_COUNT];        // byte offsets of the sections (0 = absent)
+};
+
+// Device copy of the path scalars (cosims_params plus derived values).
+struct DevParams {
+  int32_t force_type;
+  int32_t multipole_order;
+  int32_t projection;
+  int32_t charged;
+  double dt, mu, dipole_scalar, r_disp, r_mp;
+  double ell_a, ell_b, ell_c, max_rad;
+  double b_max, start_dist, g_min, g_max, vdist_a, vdist_norm, vdist_max;
+  double ccs_const;
+  int64_t max_steps;
+};
+
+enum RunMode : int { MODE_LIST = 0, MODE_SAMPLED = 1 };
+
+// Device-side counters of one run (all 64-bit, summed with atomics).
+enum Counter : int {
+  C_STEPS = 0,      // integration steps, all attempts
+  C_FORCE_EVALS,    // acceleration evaluations
+  C_POT_EVALS,      // potential evaluations
+  C_PAIR_LJ,        // LJ-only pair terms
+  C_PAIR_ES,        // electrostatic (+LJ) pair terms
+  C_PAIR_POT,       // potential pair terms
+  C_FAR,            // far-field cluster terms
+  C_ERROR,          // error flags (bit 0: staging wait gave up)
+  C_COUNT
+};
+
+struct TrajArgs {
+  MolImage img;          // the image staged into shared memory
+  MolImage img64;        // F64 image (global) used for the energy check
+  DevParams par;
+  int32_t mode;          // RunMode
+  int32_t group_lanes;   // lanes per trajectory (power of two, <= 32)
+  int32_t use_smem;      // image staged in shared memory (else read from global)
+  int32_t mode_stride;   // bytes of per-group cluster-mode scratch in shared memory
+  const double *pos0;    // MODE_LIST: 3n start positions
+  const double *vel0;    // MODE_LIST: 3n start velocities
+  uint64_t seed;         // MODE_SAMPLED
+  int64_t first_index;   // MODE_SAMPLED
+  int64_t n;
+  cosims_traj_out *out;  // n records
+  cosims_traj_in *inputs;// optional sampled-input records
+  unsigned long long *queue;     // work counter (reset to 0 before launch)
+  unsigned long long *counters;  // C_COUNT counters
+};
+
+// Host helpers implemented in the .cu files.
+int plain_launch(const TrajArgs &a, int block, int grid, size_t smem, void *stream);
+int mixed_launch(const TrajArgs &a, int block, int grid, size_t smem, void *stream);
+int plain_max_smem_per_block();
+int sample_launch(const DevParams &par, uint64_t seed, int64_t first, int64_t n,
+                  cosims_traj_in *inputs, double *pos0, double *vel0, int32_t *hit,
+                  void *stream);
+
+// Reduction of per-trajectory records into a cosims_ccs_sums (device).
+int reduce_launch(const cosims_traj_out *recs, int64_t n, double ccs_const,
+                  int half_angle, int64_t update_every, const unsigned long long *counters,
+                  cosims_ccs_sums *d_sums, double *scratch, int64_t scratch_len,
+                  void *stream);
+int64_t reduce_scratch_len(int64_t n);
+
+}  // namespace cosims

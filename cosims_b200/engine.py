@@ -1,0 +1,185 @@
+"""Python binding of the CCS engine's C ABI (include/cosims_cuda.h).
+
+`Context` mirrors the reference's per-molecule trajectory driver (monteTraj,
+monteTraj.cpp:26-502): it owns one molecule on the device and runs batches of
+trajectories through the CUDA kernels.  There is no CPU path: if the CUDA
+library or a B200 is missing, every call raises `CosimsError`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_DIR = os.path.join(HERE, "_lib")
+LIB_PATH = os.path.join(LIB_DIR, "libcosims_cuda.so")
+
+_LIB = None
+_LOCK = threading.Lock()
+
+
+class CosimsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"cosims status {status}: {message}")
+        self.status = status
+
+
+def lib():
+    """Load libcosims_cuda.so (built by cosims_b200.build.build())."""
+    global _LIB
+    with _LOCK:
+        if _LIB is None:
+            if not os.path.exists(LIB_PATH):
+                raise CosimsError(abi.ERR_UNSUPPORTED,
+                                  f"CUDA library missing: {LIB_PATH} (run the build)")
+            L = C.CDLL(LIB_PATH)
+            P, V = C.POINTER, C.c_void_p
+            st = C.c_int
+            sig = {
+                "cosims_abi_version": (C.c_int32, []),
+                "cosims_last_error": (C.c_char_p, []),
+                "cosims_device_count": (C.c_int32, []),
+                "cosims_ctx_create": (st, [P(abi.Molecule), P(abi.Params), C.c_int32, C.c_int32,
+                                           P(V)]),
+                "cosims_ctx_destroy": (None, [V]),
+                "cosims_ctx_set_launch": (st, [V, C.c_int32, C.c_int32]),
+                "cosims_ctx_get_launch": (st, [V, P(C.c_int32), P(C.c_int32)]),
+                "cosims_run_list": (st, [V, V, V, C.c_int64, V, V]),
+                "cosims_run_list_device": (st, [V, V, V, C.c_int64, V, V]),
+                "cosims_run_sampled": (st, [V, C.c_uint64, C.c_int64, C.c_int64, C.c_int64,
+                                            P(abi.CcsSums), V, V, V]),
+                "cosims_run_sampled_device": (st, [V, C.c_uint64, C.c_int64, C.c_int64,
+                                                   C.c_int64, V, V]),
+                "cosims_sample_inputs": (st, [V, C.c_uint64, C.c_int64, C.c_int64, V, V, V, V,
+                                              V]),
+                "cosims_batch_create": (st, [V, V, C.c_int32, C.c_int32, C.c_int32, P(V)]),
+                "cosims_batch_destroy": (None, [V]),
+                "cosims_batch_autotune": (st, [V, V]),
+                "cosims_batch_run": (st, [V, V, V, V, V, V]),
+                "cosims_batch_run_async": (st, [V, V, V, V, V, V]),
+                "cosims_batch_get_launch": (st, [V, C.c_int32, P(C.c_int32), P(C.c_int32)]),
+            }
+            for name, (res, args) in sig.items():
+                f = getattr(L, name)
+                f.restype = res
+                f.argtypes = args
+            if L.cosims_abi_version() != abi.ABI_VERSION:
+                raise CosimsError(abi.ERR_UNSUPPORTED, "ABI version mismatch")
+            _LIB = L
+    return _LIB
+
+
+def check(status: int) -> None:
+    if status != abi.OK:
+        msg = lib().cosims_last_error()
+        raise CosimsError(status, msg.decode() if msg else "")
+
+
+def device_count() -> int:
+    return int(lib().cosims_device_count())
+
+
+def _stream_ptr(stream) -> C.c_void_p:
+    if stream is None:
+        return C.c_void_p(0)
+    if isinstance(stream, int):
+        return C.c_void_p(stream)
+    return C.c_void_p(int(stream.cuda_stream))     # torch.cuda.Stream
+
+
+class Context:
+    """One molecule resident on the device (plain FP64 or mixed precision)."""
+
+    def __init__(self, mol: abi.MoleculeArrays, par: abi.Params,
+                 precision: int = abi.PLAIN_F64, device: int = 0):
+        self.mol = mol
+        self.par = par
+        self.precision = precision
+        self.device = device
+        self._view = mol.view()
+        h = C.c_void_p()
+        check(lib().cosims_ctx_create(C.byref(self._view), C.byref(par), precision, device,
+                                      C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            lib().cosims_ctx_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    def set_launch(self, group_lanes: int = 0, block_threads: int = 0) -> None:
+        check(lib().cosims_ctx_set_launch(self._h, group_lanes, block_threads))
+
+    def get_launch(self) -> tuple:
+        g, b = C.c_int32(), C.c_int32()
+        check(lib().cosims_ctx_get_launch(self._h, C.byref(g), C.byref(b)))
+        return g.value, b.value
+
+    def run_list(self, pos0: np.ndarray, vel0: np.ndarray, stream=None) -> np.ndarray:
+        """verletVel on each start state; returns TRAJ_OUT_DTYPE records."""
+        pos0 = np.ascontiguousarray(pos0, dtype=np.float64).reshape(-1, 3)
+        vel0 = np.ascontiguousarray(vel0, dtype=np.float64).reshape(-1, 3)
+        out = np.zeros(pos0.shape[0], dtype=abi.TRAJ_OUT_DTYPE)
+        check(lib().cosims_run_list(self._h, abi.vptr(pos0), abi.vptr(vel0), pos0.shape[0],
+                                    abi.vptr(out), _stream_ptr(stream)))
+        return out
+
+    def run_list_device(self, d_pos0: int, d_vel0: int, n: int, d_out: int, stream=None) -> None:
+        check(lib().cosims_run_list_device(self._h, C.c_void_p(d_pos0), C.c_void_p(d_vel0), n,
+                                           C.c_void_p(d_out), _stream_ptr(stream)))
+
+    def run_sampled(self, seed: int, first: int, n: int, update_every: int = 0,
+                    want_records: bool = False, stream=None):
+        """One CCS integral of n sampled trajectories.  Returns (sums, inputs, outs)."""
+        s = abi.CcsSums()
+        ins = np.zeros(n, abi.TRAJ_IN_DTYPE) if want_records else None
+        outs = np.zeros(n, abi.TRAJ_OUT_DTYPE) if want_records else None
+        check(lib().cosims_run_sampled(
+            self._h, seed, first, n, update_every, C.byref(s),
+            abi.vptr(ins) if ins is not None else None,
+            abi.vptr(outs) if outs is not None else None, _stream_ptr(stream)))
+        return s, ins, outs
+
+    def run_sampled_device(self, seed: int, first: int, n: int, update_every: int,
+                           d_sums: int, stream=None) -> None:
+        check(lib().cosims_run_sampled_device(self._h, seed, first, n, update_every,
+                                              C.c_void_p(d_sums), _stream_ptr(stream)))
+
+    def sample_inputs(self, seed: int, first: int, n: int, stream=None):
+        ins = np.zeros(n, abi.TRAJ_IN_DTYPE)
+        pos0, vel0 = np.zeros((n, 3)), np.zeros((n, 3))
+        hit = np.zeros(n, np.int32)
+        check(lib().cosims_sample_inputs(self._h, seed, first, n, abi.vptr(ins), abi.vptr(pos0),
+                                         abi.vptr(vel0), abi.vptr(hit), _stream_ptr(stream)))
+        return ins, pos0, vel0, hit
+
+
+def omega(s: abi.CcsSums) -> tuple:
+    """Omega and its standard error for one integral (monteTraj.cpp:381-387)."""
+    n = float(s.n_eff)
+    if n <= 0:
+        return float("nan"), float("nan")
+    m = s.sum / n
+    var = s.sum2 / n - m * m
+    return m, float(np.sqrt(max(var, 0.0) / n))

@@ -109,14 +109,16 @@ typedef struct cosims_params {
     double vdist_norm;        /* renormalised g^5 exp(-a g^2) normalisation     */
     double vdist_max;         /* density at the mode (maxVelDistr)              */
     double ccs_const;         /* const1 * const2 (monteTraj.cpp:91-94, :472)    */
-    int64_t max_steps;        /* hard cap on integration steps per trajectory;
-                                 the reference has none (0 = default 2^22)      */
+    int64_t max_steps;        /* hard cap on integration steps per trajectory
+                                 (0 = default 2^18); the reference has none.  A
+                                 capped or non-finite trajectory is a failure
+                                 with COSIMS_TRAJ_STEPCAP set                   */
 } cosims_params;
 
 /* Per-trajectory status bits. */
 #define COSIMS_TRAJ_HIT       0x1u  /* start state reached the ellipsoid        */
 #define COSIMS_TRAJ_SUCCESS   0x2u  /* verletVel returned true                  */
-#define COSIMS_TRAJ_STEPCAP   0x4u  /* stopped by max_steps (counted as failed) */
+#define COSIMS_TRAJ_STEPCAP   0x4u  /* stopped by max_steps or a non-finite state */
 #define COSIMS_TRAJ_ETRIES_SHIFT 8  /* bits 8..15: energy-check retries         */
 #define COSIMS_TRAJ_OTRIES_SHIFT 16 /* bits 16..23: orbit-detector dt shrinks   */
 
@@ -148,7 +150,14 @@ typedef struct cosims_ccs_sums {
                              still holds at the end (monteTraj.cpp:380-381,
                              504-521); see cosims_run_sampled                   */
     int64_t steps;        /* integration steps, all attempts                     */
-    int64_t pair_evals;   /* atom-pair interactions evaluated (roofline work)    */
+    /* Work done, for the roofline: acceleration and potential evaluations and
+     * the pair terms they summed, by kind. */
+    int64_t force_evals;
+    int64_t pot_evals;
+    int64_t pair_lj;      /* Lennard-Jones-only pair terms                       */
+    int64_t pair_es;      /* pair terms with the charge field (+ LJ if in range) */
+    int64_t pair_pot;     /* potential pair terms (energy check)                 */
+    int64_t far_terms;    /* cluster multipole far-field terms                   */
 } cosims_ccs_sums;
 
 typedef struct cosims_ctx cosims_ctx;

@@ -386,8 +386,9 @@ static double angle3(const double a[3], const double b[3])
 
 /* diffEqSolver::verletVel (diffEqSolver.cpp:81-211).  Besides chi, the
  * return value and stepCount it reports the retry counts and stops at
- * par->max_steps (the reference has no cap; the cap is far above any
- * trajectory it finishes). */
+ * par->max_steps (default 2^18) or when the state turns non-finite; the
+ * reference has neither stop (it would loop), and no trajectory it finishes
+ * comes near the cap. */
 void oracle_verlet(const cosims_molecule *mol, const cosims_params *par,
                    const double initPos[3], const double initVel[3],
                    cosims_traj_out *out)
@@ -395,7 +396,7 @@ void oracle_verlet(const cosims_molecule *mol, const cosims_params *par,
     const double a = par->ell_a, b = par->ell_b, c = par->ell_c;
     const double maxRad = fmax(a, fmax(b, c));
     const double time = par->dt;
-    const int64_t cap = par->max_steps > 0 ? par->max_steps : ((int64_t)1 << 22);
+    const int64_t cap = par->max_steps > 0 ? par->max_steps : ((int64_t)1 << 18);
     double maxTries = 8, trajTries = 0;
     double dt = time;
     double rDot_new = 0, rDot_old = 0, orbits = 0;
@@ -460,7 +461,7 @@ void oracle_verlet(const cosims_molecule *mol, const cosims_params *par,
                 }
             }
         }
-        if (total_steps >= cap) {
+        if (total_steps >= cap || !isfinite(rDot_new)) {
             out->chi = ORACLE_PI_2;
             out->steps = stepCount;
             out->status = COSIMS_TRAJ_HIT | COSIMS_TRAJ_STEPCAP |

@@ -263,16 +263,18 @@ void ref_run_list(int n, const double *pos0, const double *vel0, double *chi,
     }
 }
 
-/* monteTraj::setUpTraj (monteTraj.cpp:174-278) driven by a seeded
- * mt19937_64; returns the sampled (b, phi, theta, gamma, g), the start state
- * and whether the ellipsoid was hit.  srand(seed) fixes rand()'s gCheck. */
-void ref_sample(int n, unsigned long long seed, double *bpgtg, double *pos0,
-                double *vel0, int *hit)
+/* monteTraj::setUpTraj (monteTraj.cpp:174-278) driven by mt19937_64(seed),
+ * as thread 0 of the reference's first integral draws it
+ * (monteTraj.cpp:344-349); returns the sampled (b, phi, theta, gamma, g), the
+ * start state and whether the ellipsoid was hit.  rand() (gCheck) is reset
+ * to srand(rand_seed); the reference never seeds it, which is srand(1). */
+void ref_sample(int n, unsigned long long seed, unsigned rand_seed, double *bpgtg,
+                double *pos0, double *vel0, int *hit)
 {
     monteTraj &m = *g_monte;
     std::mt19937_64 gen(seed);
     std::uniform_real_distribution<double> distr(0.0, 1.0);
-    std::srand((unsigned)seed);
+    std::srand(rand_seed);
     bool saved = printData_ext;
     printData_ext = true;
     for (int i = 0; i < n; i++) {

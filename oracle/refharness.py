@@ -56,7 +56,7 @@ def lib():
         L.ref_force.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
         L.ref_potential.argtypes = [C.c_int, C.c_void_p, C.c_void_p]
         L.ref_run_list.argtypes = [C.c_int] + [C.c_void_p] * 6
-        L.ref_sample.argtypes = [C.c_int, C.c_ulonglong] + [C.c_void_p] * 4
+        L.ref_sample.argtypes = [C.c_int, C.c_ulonglong, C.c_uint] + [C.c_void_p] * 4
         _LIB = L
     return _LIB
 
@@ -150,12 +150,12 @@ class RefSetup:
                            abi.vptr(steps), abi.vptr(de))
         return chi, succ, steps, de
 
-    def sample(self, n: int, seed: int):
+    def sample(self, n: int, seed: int, rand_seed: int = 1):
         """monteTraj::setUpTraj driven by mt19937_64(seed): inputs, start states, hits."""
         vals = np.zeros((n, 5))
         pos0, vel0 = np.zeros((n, 3)), np.zeros((n, 3))
         hit = np.zeros(n, np.int32)
-        lib().ref_sample(n, seed, abi.vptr(vals), abi.vptr(pos0), abi.vptr(vel0), abi.vptr(hit))
+        lib().ref_sample(n, seed, rand_seed, abi.vptr(vals), abi.vptr(pos0), abi.vptr(vel0), abi.vptr(hit))
         inputs = np.zeros(n, abi.TRAJ_IN_DTYPE)
         for i, k in enumerate(("b", "phi", "theta", "gamma", "g")):
             inputs[k] = vals[:, i]
