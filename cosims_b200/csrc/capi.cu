@@ -271,9 +271,8 @@ cosims_status launch_shape(const cosims_ctx *c, int64_t n, LaunchShape &ls) {
   return COSIMS_OK;
 }
 
-cosims_status run_core(cosims_ctx *c, int mode, const double *d_pos0, const double *d_vel0,
-                       uint64_t seed, int64_t first, int64_t n, cosims_traj_out *d_out,
-                       cosims_traj_in *d_in, void *stream) {
+cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0,
+                       const int32_t *d_hit, int64_t n, cosims_traj_out *d_out, void *stream) {
   LaunchShape ls;
   cosims_status st = launch_shape(c, n, ls);
   if (st != COSIMS_OK) return st;
@@ -288,23 +287,36 @@ cosims_status run_core(cosims_ctx *c, int mode, const double *d_pos0, const doub
   a.img = plain ? c->img64 : c->img32;
   a.img64 = c->img64;
   a.par = c->par;
-  a.mode = mode;
   a.group_lanes = plain ? 1 : c->group_lanes;
   a.use_smem = ls.use_smem;
   a.mode_stride = ls.mode_stride;
   a.pos0 = d_pos0;
   a.vel0 = d_vel0;
-  a.seed = seed;
-  a.first_index = first;
+  a.hit = d_hit;
   a.n = n;
   a.out = d_out;
-  a.inputs = d_in;
   a.queue = c->d_queue;
   a.counters = c->d_counters;
   int rc = plain ? plain_launch(a, ls.block, ls.grid, ls.smem, stream)
                  : mixed_launch(a, ls.block, ls.grid, ls.smem, stream);
   if (rc != 0) return cuda_fail((cudaError_t)rc, "trajectory kernel launch");
   c->last_shape = ls;
+  return COSIMS_OK;
+}
+
+// Start states of trajectories first..first+n-1 into the context's buffers
+// (one sampler kernel: the trajectory kernels only read them).
+cosims_status sample_into(cosims_ctx *c, uint64_t seed, int64_t first, int64_t n,
+                          bool keep_inputs, void *stream) {
+  cosims_status st = grow(&c->d_out, &c->out_cap, n);
+  if (st == COSIMS_OK) st = grow(&c->d_in, &c->in_cap, n);
+  if (st == COSIMS_OK) st = grow(&c->d_pos0, &c->list_cap, 3 * n);
+  if (st == COSIMS_OK) st = grow(&c->d_vel0, &c->vel_cap, 3 * n);
+  if (st == COSIMS_OK) st = grow(&c->d_hit, &c->hit_cap, n);
+  if (st != COSIMS_OK) return st;
+  (void)keep_inputs;
+  int rc = sample_launch(c->par, seed, first, n, c->d_in, c->d_pos0, c->d_vel0, c->d_hit, stream);
+  if (rc != 0) return cuda_fail((cudaError_t)rc, "sampler launch");
   return COSIMS_OK;
 }
 
@@ -407,8 +419,9 @@ cosims_status cosims_ctx_set_launch(cosims_ctx *c, int32_t group_lanes, int32_t 
     c->group_lanes = group_lanes;
   }
   if (block_threads) {
-    if (block_threads < 32 || block_threads > 256 || (block_threads & 31))
-      return fail(COSIMS_ERR_INVALID, "block_threads must be a multiple of 32 in 32..256");
+    const int maxb = c->precision == COSIMS_PRECISION_PLAIN_F64 ? 128 : 256;
+    if (block_threads < 32 || block_threads > maxb || (block_threads & 31))
+      return fail(COSIMS_ERR_INVALID, "block_threads must be a multiple of 32 in 32..%d", maxb);
     c->block_threads = block_threads;
   }
   if (c->block_threads < c->group_lanes)
@@ -431,7 +444,7 @@ cosims_status cosims_run_list_device(cosims_ctx *c, const double *d_pos0, const 
   if (n > 0 && (!d_pos0 || !d_vel0 || !d_out))
     return fail(COSIMS_ERR_INVALID, "pos0, vel0 and out are required");
   DeviceGuard g(c->device);
-  return run_core(c, MODE_LIST, d_pos0, d_vel0, 0, 0, n, d_out, nullptr, stream);
+  return run_core(c, d_pos0, d_vel0, nullptr, n, d_out, stream);
 }
 
 cosims_status cosims_run_list(cosims_ctx *c, const double *pos0, const double *vel0, int64_t n,
@@ -450,7 +463,7 @@ cosims_status cosims_run_list(cosims_ctx *c, const double *pos0, const double *v
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(c->d_vel0, vel0, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return cuda_fail(e, "copy of start states");
-  st = run_core(c, MODE_LIST, c->d_pos0, c->d_vel0, 0, 0, n, c->d_out, nullptr, stream);
+  st = run_core(c, c->d_pos0, c->d_vel0, nullptr, n, c->d_out, stream);
   if (st != COSIMS_OK) return st;
   e = cudaMemcpyAsync(out, c->d_out, sizeof(cosims_traj_out) * n, cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return cuda_fail(e, "copy of results");
@@ -464,9 +477,9 @@ cosims_status cosims_run_sampled_device(cosims_ctx *c, uint64_t seed, int64_t fi
   if (n < 0 || first < 0) return fail(COSIMS_ERR_INVALID, "n and first_index must be >= 0");
   if (!d_sums) return fail(COSIMS_ERR_INVALID, "sums is NULL");
   DeviceGuard g(c->device);
-  cosims_status st = grow(&c->d_out, &c->out_cap, n);
+  cosims_status st = sample_into(c, seed, first, n, false, stream);
   if (st != COSIMS_OK) return st;
-  st = run_core(c, MODE_SAMPLED, nullptr, nullptr, seed, first, n, c->d_out, nullptr, stream);
+  st = run_core(c, c->d_pos0, c->d_vel0, c->d_hit, n, c->d_out, stream);
   if (st != COSIMS_OK) return st;
   int rc = reduce_launch(c->d_out, n, c->par.ccs_const,
                          c->precision == COSIMS_PRECISION_MIXED ? 1 : 0, update_every,
@@ -482,11 +495,9 @@ cosims_status cosims_run_sampled(cosims_ctx *c, uint64_t seed, int64_t first, in
   if (!sums) return fail(COSIMS_ERR_INVALID, "sums is NULL");
   if (n < 0 || first < 0) return fail(COSIMS_ERR_INVALID, "n and first_index must be >= 0");
   DeviceGuard g(c->device);
-  cosims_status st = grow(&c->d_out, &c->out_cap, n);
-  if (st == COSIMS_OK && inputs) st = grow(&c->d_in, &c->in_cap, n);
+  cosims_status st = sample_into(c, seed, first, n, true, stream);
   if (st != COSIMS_OK) return st;
-  st = run_core(c, MODE_SAMPLED, nullptr, nullptr, seed, first, n, c->d_out,
-                inputs ? c->d_in : nullptr, stream);
+  st = run_core(c, c->d_pos0, c->d_vel0, c->d_hit, n, c->d_out, stream);
   if (st != COSIMS_OK) return st;
   int rc = reduce_launch(c->d_out, n, c->par.ccs_const,
                          c->precision == COSIMS_PRECISION_MIXED ? 1 : 0, update_every,
@@ -511,14 +522,9 @@ cosims_status cosims_sample_inputs(cosims_ctx *c, uint64_t seed, int64_t first, 
   if (!inputs || !pos0 || !vel0 || !hit)
     return fail(COSIMS_ERR_INVALID, "inputs, pos0, vel0 and hit are required");
   DeviceGuard g(c->device);
-  cosims_status st = grow(&c->d_in, &c->in_cap, n);
-  if (st == COSIMS_OK) st = grow(&c->d_pos0, &c->list_cap, 3 * n);
-  if (st == COSIMS_OK) st = grow(&c->d_vel0, &c->vel_cap, 3 * n);
-  if (st == COSIMS_OK) st = grow(&c->d_hit, &c->hit_cap, n);
+  cosims_status st = sample_into(c, seed, first, n, true, stream);
   if (st != COSIMS_OK) return st;
   cudaStream_t s = (cudaStream_t)stream;
-  int rc = sample_launch(c->par, seed, first, n, c->d_in, c->d_pos0, c->d_vel0, c->d_hit, stream);
-  if (rc != 0) return cuda_fail((cudaError_t)rc, "sampler launch");
   cudaError_t e = cudaMemcpyAsync(inputs, c->d_in, sizeof(cosims_traj_in) * n, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(pos0, c->d_pos0, 24 * n, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaMemcpyAsync(vel0, c->d_vel0, 24 * n, cudaMemcpyDeviceToHost, s);

@@ -88,8 +88,6 @@ struct DevParams {
   int64_t max_steps;
 };
 
-enum RunMode : int { MODE_LIST = 0, MODE_SAMPLED = 1 };
-
 // Device-side counters of one run (all 64-bit, summed with atomics).
 enum Counter : int {
   C_STEPS = 0,      // integration steps, all attempts
@@ -107,17 +105,15 @@ struct TrajArgs {
   MolImage img;          // the image staged into shared memory
   MolImage img64;        // F64 image (global) used for the energy check
   DevParams par;
-  int32_t mode;          // RunMode
   int32_t group_lanes;   // lanes per trajectory (power of two, <= 32)
   int32_t use_smem;      // image staged in shared memory (else read from global)
   int32_t mode_stride;   // bytes of per-group cluster-mode scratch in shared memory
-  const double *pos0;    // MODE_LIST: 3n start positions
-  const double *vel0;    // MODE_LIST: 3n start velocities
-  uint64_t seed;         // MODE_SAMPLED
-  int64_t first_index;   // MODE_SAMPLED
+  int32_t pad0;
+  const double *pos0;    // 3n start positions
+  const double *vel0;    // 3n start velocities
+  const int32_t *hit;    // n ellipsoid hits (NULL: every start state is a hit)
   int64_t n;
   cosims_traj_out *out;  // n records
-  cosims_traj_in *inputs;// optional sampled-input records
   unsigned long long *queue;     // work counter (reset to 0 before launch)
   unsigned long long *counters;  // C_COUNT counters
 };

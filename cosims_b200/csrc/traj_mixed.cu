@@ -311,18 +311,16 @@ __global__ void __launch_bounds__(256) traj_mixed_kernel(const TrajArgs a) {
         if (lane == 0) tk = (long long)atomicAdd(a.queue, 1ull);
         t = __shfl_sync(gmask, tk, 0, G);
         if (t >= a.n) { phase = P_DONE; break; }
-        if (a.mode == MODE_LIST) {
-          for (int i = 0; i < 3; i++) { p0[i] = a.pos0[3 * t + i]; v0[i] = a.vel0[3 * t + i]; }
-          phase = P_INIT_FIRST;
-          break;
+        if (a.hit && !a.hit[t]) {                 // ellipsoid miss: chi = 0
+          if (lane == 0) {
+            cosims_traj_out o = {0.0, 0.0, 0, 0u};
+            a.out[t] = o;
+          }
+          continue;
         }
-        cosims_traj_in in = sample_inputs(p, a.seed, (uint64_t)(a.first_index + t));
-        if (a.inputs && lane == 0) a.inputs[t] = in;
-        if (start_state(p, in, p0, v0)) { phase = P_INIT_FIRST; break; }
-        if (lane == 0) {
-          cosims_traj_out o = {0.0, 0.0, 0, 0u};
-          a.out[t] = o;
-        }
+        for (int i = 0; i < 3; i++) { p0[i] = a.pos0[3 * t + i]; v0[i] = a.vel0[3 * t + i]; }
+        phase = P_INIT_FIRST;
+        break;
       }
       if (phase == P_INIT_FIRST) {
         tries = 0; maxTries = 8; dt = p.dt; step = 0; total = 0; etries = 0; otries = 0;

@@ -357,7 +357,7 @@ __device__ __forceinline__ double angle3(const double a[3], const double b[3]) {
 
 enum Phase : int { P_ACQUIRE = 0, P_INIT_FIRST, P_INIT_RETRY, P_STEP, P_DONE };
 
-__global__ void __launch_bounds__(256) traj_plain_kernel(const TrajArgs a) {
+__global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
   const unsigned char *base = a.img.gbase;
@@ -394,16 +394,14 @@ __global__ void __launch_bounds__(256) traj_plain_kernel(const TrajArgs a) {
       for (;;) {
         t = (long long)atomicAdd(a.queue, 1ull);
         if (t >= a.n) { phase = P_DONE; break; }
-        if (a.mode == MODE_LIST) {
-          for (int i = 0; i < 3; i++) { p0[i] = a.pos0[3 * t + i]; v0[i] = a.vel0[3 * t + i]; }
-          phase = P_INIT_FIRST;
-          break;
+        if (a.hit && !a.hit[t]) {                 // ellipsoid miss: chi = 0
+          cosims_traj_out o = {0.0, 0.0, 0, 0u};
+          a.out[t] = o;
+          continue;
         }
-        cosims_traj_in in = sample_inputs(p, a.seed, (uint64_t)(a.first_index + t));
-        if (a.inputs) a.inputs[t] = in;
-        if (start_state(p, in, p0, v0)) { phase = P_INIT_FIRST; break; }
-        cosims_traj_out o = {0.0, 0.0, 0, 0u};    // ellipsoid miss: chi = 0
-        a.out[t] = o;
+        for (int i = 0; i < 3; i++) { p0[i] = a.pos0[3 * t + i]; v0[i] = a.vel0[3 * t + i]; }
+        phase = P_INIT_FIRST;
+        break;
       }
       if (phase == P_INIT_FIRST) {
         tries = 0; maxTries = 8; dt = p.dt; step = 0; total = 0; etries = 0; otries = 0;

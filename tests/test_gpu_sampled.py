@@ -72,11 +72,7 @@ def test_sampled_sums_deterministic_across_launch_shapes(precision):
     mol, par, _ = load("c0_t5")
     with engine.Context(mol, par, precision) as ctx:
         s1, _, o1 = ctx.run_sampled(seed=9, first=0, n=3000, update_every=1000, want_records=True)
-        if precision == abi.MIXED:
-            g, _ = ctx.get_launch()
-            ctx.set_launch(group_lanes=g, block_threads=64)
-        else:
-            ctx.set_launch(block_threads=64)
+        ctx.set_launch(block_threads=64)
         s2, _, o2 = ctx.run_sampled(seed=9, first=0, n=3000, update_every=1000, want_records=True)
     np.testing.assert_array_equal(o1, o2)
     assert s1.sum == s2.sum and s1.sum2 == s2.sum2 and s1.n_eff == s2.n_eff
