@@ -1,0 +1,381 @@
+#!/usr/bin/env python
+"""Trajectory-method CCS throughput on B200.
+
+Workload (one step = one CCS integral): the 512-atom synthetic ion of the
+benchmark's second configuration (charge +2, partial charges N(0, 0.3 e),
+exact induced-dipole electrostatics with the LJ cluster cut-off, force
+variant 3), 100 000 sampled trajectories per step, He at 298 K.  The timed
+form is the mixed-precision engine (FP32 pair forces, FP64 integration and
+energy check); the plain FP64 form runs on the same sampled inputs to give
+the CCS error of mixed against FP64 and the plain throughput.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  Under torchrun every rank integrates its own
+trajectories (disjoint Philox counter ranges; weak scaling) and the time is
+the max over ranks.  --impl reference times the unmodified reference program
+(oracle/_ref/cosims, built from the reference sources) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "trajectories/s at <=0.3% CCS err (mixed vs plain FP64); p50/p99 request latency"
+UNIT = "trajectories/s"
+N_TRAJ = 100_000
+SEED = 20251203
+# Algorithmic FP32 work per pair term, from the reference's formulas
+# (forceAccel.cpp:856-884 LJ; :751-805 LJ + charge field and gradient):
+# flops with FMA = 2, division and square root = 1.
+FLOPS_LJ, FLOPS_ES, FLOPS_FAR = 22, 55, 60
+FLOPS_POT_CHARGED, FLOPS_POT_NEUTRAL = 24, 15
+
+
+def cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def workload_files(tmp: str):
+    from cosims_b200 import synth
+    mol = synth.config1_molecule()
+    mp, ip = synth.write_case(tmp, mol, "cutoff", traj_thousands=N_TRAJ / 1000, iterations=1)
+    return mol, mp, ip
+
+
+# ---- clocks during the timed region ----------------------------------------------------
+
+class ClockSampler:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+             "-i", str(self.device), "-lms", "200"],
+            stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        time.sleep(0.3)
+
+    def stop(self) -> dict:
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9 and f[1].isdigit():
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [int(r[1]) for r in rows]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": int(rows[0][2]),
+                "reasons": reasons, "samples": len(rows),
+                "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())
+                if any(r[3].replace(".", "").isdigit() for r in rows) else None}
+
+
+# ---- the reference program on the host cores ------------------------------------------
+
+def reference_binary() -> str | None:
+    p = os.path.join(ROOT, "oracle", "_ref", "cosims")
+    return p if os.path.exists(p) and os.access(p, os.X_OK) else None
+
+
+def run_reference(mp: str, traj: int, iters: int, threads: int, seed: int = SEED,
+                  timeout: float = 1800) -> list:
+    """Runs the unmodified reference program; returns per-integral trajectory
+    phase times (its `Total time:` lines are cumulative, monteTraj.cpp:397)."""
+    from cosims_b200 import synth
+    work = tempfile.mkdtemp(prefix="cosims_refbench_")
+    ip = os.path.join(work, "bench.in")
+    with open(ip, "w") as f:
+        f.write(synth.input_text("cutoff", traj_thousands=traj / 1000, iterations=iters,
+                                 extra={"threads": threads, "print_rate": traj}, name="bench"))
+    subprocess.run([reference_binary(), "-m", mp, "-i", ip, "-s", str(seed)], cwd=work,
+                   check=True, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                   timeout=timeout)
+    logs = [f for f in os.listdir(work) if f.startswith("omega_")]
+    text = open(os.path.join(work, logs[0])).read()
+    cum = [float(x) for x in re.findall(r"Total time: ([0-9.]+);", text)]
+    shutil.rmtree(work, ignore_errors=True)
+    return [b - a for a, b in zip([0.0] + cum[:-1], cum)]
+
+
+def reference_sample_size(target_s: float, ncores: int) -> int:
+    per_core = 550.0     # trajectories/s per core of the reference on this workload
+    n = int(round(per_core * ncores * target_s / 1000.0)) * 1000
+    return max(1000, min(N_TRAJ, n))
+
+
+def reference_arm(args, rank: int) -> None:
+    if rank != 0:
+        return
+    if not reference_binary():
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference program not built (oracle/_ref/cosims)"}))
+        return
+    tmp = tempfile.mkdtemp(prefix="cosims_bench_")
+    _, mp, _ = workload_files(tmp)
+    nc = cores()
+    traj = reference_sample_size(3.0, nc)
+    times = run_reference(mp, traj, args.warmup + args.steps, nc)
+    timed = times[args.warmup:]
+    value = traj * len(timed) / sum(timed)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000 * sum(timed) / len(timed), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": config_block(group_lanes=None, l2="n/a (host CPU)"),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nc, "kind": "reference",
+                         "sample": f"{traj} trajectories per integral x {args.steps} integrals "
+                                   f"(reference program, OpenMP threads = {nc})"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def config_block(group_lanes, l2) -> dict:
+    return {"workload": "512-atom synthetic ion, charge +2, force variant 3 (exact "
+                        "induced dipole + LJ cluster cut-off), He 298 K; one CCS integral "
+                        f"of {N_TRAJ} sampled trajectories per step",
+            "atoms": 512, "traj_per_step": N_TRAJ, "force_type": 3,
+            "form": "mixed (FP32 pair forces, FP64 integration and energy check)",
+            "group_lanes": group_lanes, "l2": l2}
+
+
+# ---- our arm ------------------------------------------------------------------------------
+
+def roofline_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return None
+    return None
+
+
+def autotune(ctx, stream, torch, d_sums) -> int:
+    """Lanes per trajectory for this molecule: the fastest of a short sweep."""
+    best, best_ms = None, 1e30
+    for g in (2, 4, 8, 16, 32):
+        ctx.set_launch(group_lanes=g)
+        ctx.run_sampled_device(SEED + 7, 0, 20000, 0, d_sums.data_ptr(), stream)
+        ms = ctx.kernel_ms()
+        if ms < best_ms:
+            best, best_ms = g, ms
+    ctx.set_launch(group_lanes=best)
+    return best
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank)
+        return
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from cosims_b200 import abi, engine, host
+
+    tmp = tempfile.mkdtemp(prefix="cosims_bench_")
+    _, mp, ip = workload_files(tmp)
+    st = host.setup_from_files(mp, ip, seed=SEED)
+    mol, par = st.mol, st.params
+    stream = torch.cuda.current_stream()
+    d_sums = torch.zeros(1024, dtype=torch.uint8, device="cuda")
+    step_sums = torch.zeros((args.steps, 128), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    first0 = rank * 10 ** 9          # disjoint counter range per rank
+
+    ctx = engine.Context(mol, par, abi.MIXED, device=local)
+    g = autotune(ctx, stream, torch, d_sums)
+    for w in range(args.warmup):
+        ctx.run_sampled_device(SEED, first0 + w * N_TRAJ, N_TRAJ, 0, d_sums.data_ptr(), stream)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    kern_ms = []
+    sz = abi.C.sizeof(abi.CcsSums)
+    for k in range(args.steps):
+        flush.zero_()                                   # L2 flush between steps
+        ev[k][0].record(stream)
+        ctx.run_sampled_device(SEED, first0 + (args.warmup + k) * N_TRAJ, N_TRAJ, 0,
+                               step_sums[k].data_ptr(), stream)
+        ev[k][1].record(stream)
+        kern_ms.append(ctx.kernel_ms())
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    mean_ms = sum(step_ms) / len(step_ms)
+    if dist:
+        t = torch.tensor([mean_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        mean_ms = float(t.item())
+    value = world * N_TRAJ / (mean_ms / 1000.0)
+
+    # work counters of the timed steps -> algorithmic flops of the trajectory kernel
+    raw = step_sums.cpu().numpy()
+    sums = [abi.CcsSums.from_buffer_copy(raw[k, :sz].tobytes()) for k in range(args.steps)]
+    pot_flops = FLOPS_POT_CHARGED if par.charged else FLOPS_POT_NEUTRAL
+    flops = [FLOPS_LJ * s.pair_lj + FLOPS_ES * s.pair_es + FLOPS_FAR * s.far_terms +
+             pot_flops * s.pair_pot for s in sums]
+    kmean = sum(kern_ms) / len(kern_ms)
+    achieved = sum(flops) / len(flops) / (kmean / 1000.0) / 1e12
+    fp32_peak, fp64_peak = engine.probe_peaks(local)
+    tr = roofline_traffic()
+    traffic = None
+    if tr and tr.get("bytes_per_traj"):
+        traffic = tr["bytes_per_traj"] * N_TRAJ
+
+    # CCS of the timed integrals (merged over ranks)
+    tot = np.array([sum(s.sum for s in sums), sum(s.sum2 for s in sums),
+                    float(sum(s.n_eff for s in sums))])
+    if dist:
+        t = torch.tensor(tot, device="cuda", dtype=torch.float64)
+        dist.all_reduce(t)
+        tot = t.cpu().numpy()
+    omega = tot[0] / tot[2]
+    omega_se = math.sqrt(max(tot[1] / tot[2] - omega ** 2, 0.0) / tot[2])
+
+    # plain FP64 form on identical inputs: throughput and the CCS error of mixed
+    plain = engine.Context(mol, par, abi.PLAIN_F64, device=local)
+    first_cmp = first0 + args.warmup * N_TRAJ
+    plain.run_sampled_device(SEED, first_cmp, 20000, 0, d_sums.data_ptr(), stream)  # warm
+    flush.zero_()
+    pe = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    pe[0].record(stream)
+    plain.run_sampled_device(SEED, first_cmp, N_TRAJ, 0, d_sums.data_ptr(), stream)
+    pe[1].record(stream)
+    torch.cuda.synchronize()
+    plain_ms = pe[0].elapsed_time(pe[1])
+    ps = abi.CcsSums.from_buffer_copy(d_sums.cpu().numpy()[:sz].tobytes())
+    ms0 = sums[0]
+    ccs_err = abs(ms0.sum - ps.sum) / ps.sum * 100.0
+
+    # end to end through the C ABI with host buffers: pinned start states in,
+    # per-trajectory results out, copies inside the timed region
+    _, p0, v0, hit = ctx.sample_inputs(SEED, first_cmp, N_TRAJ)
+    p0 = torch.from_numpy(np.ascontiguousarray(p0[hit == 1])).pin_memory().numpy()
+    v0 = torch.from_numpy(np.ascontiguousarray(v0[hit == 1])).pin_memory().numpy()
+    n_e2e = p0.shape[0]
+    ctx.run_list(p0, v0)
+    e2e_ms = []
+    for k in range(args.steps):
+        flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.run_list(p0, v0, stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e_mean = sum(e2e_ms) / len(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e_mean], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_mean = float(t.item())
+    e2e_value = world * n_e2e / (e2e_mean / 1000.0)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and reference_binary():
+        nc = cores()
+        traj = reference_sample_size(10.0, nc)
+        t = run_reference(mp, traj, 1, nc)
+        cpu = {"value": traj / t[0], "unit": UNIT, "cores": nc, "kind": "reference",
+               "sample": f"one integral of {traj} trajectories of the same molecule and "
+                         f"input (reference program, OpenMP threads = {nc})"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 pair forces / fp64 integration", "data": "synthetic",
+            "config": config_block(g, "flushed between steps (512 MiB write)"),
+            "ccs": {"omega_A2": omega, "se_A2": omega_se,
+                    "err_pct_mixed_vs_plain": ccs_err, "bar_pct": 0.3},
+            "plain_f64": {"value": N_TRAJ / (plain_ms / 1000.0), "ms_per_step": plain_ms},
+            "mixed_over_plain": value / world / (N_TRAJ / (plain_ms / 1000.0)),
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
+                         "kernel": "traj_mixed_kernel<3>",
+                         "kernel_ms": kmean,
+                         "peak_source": "measured in this run: FP32 FMA chains "
+                                        "(cosims_probe_peaks); the driver's peaks file holds "
+                                        "only HBM and bf16 tensor figures",
+                         "fp64_peak": fp64_peak},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 48 * n_e2e,
+                    "d2h_bytes_per_step": 24 * n_e2e,
+                    "path": "cosims_run_list: pinned host start states -> device -> host "
+                            "per-trajectory records"},
+            "gpu_launches": 4 * args.steps,
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+    ctx.close()
+    plain.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -297,9 +297,17 @@ cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0
   a.out = d_out;
   a.queue = c->d_queue;
   a.counters = c->d_counters;
+  if (!c->ev0) {
+    e = cudaEventCreate(&c->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaEventCreate");
+  }
+  cudaEventRecord(c->ev0, s);
   int rc = plain ? plain_launch(a, ls.block, ls.grid, ls.smem, stream)
                  : mixed_launch(a, ls.block, ls.grid, ls.smem, stream);
   if (rc != 0) return cuda_fail((cudaError_t)rc, "trajectory kernel launch");
+  cudaEventRecord(c->ev1, s);
+  c->timed = true;
   c->last_shape = ls;
   return COSIMS_OK;
 }
@@ -406,7 +414,19 @@ void cosims_ctx_destroy(cosims_ctx *c) {
   cudaFree(c->d_vel0);
   cudaFree(c->d_red);
   cudaFree(c->d_hit);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
   delete c;
+}
+
+cosims_status cosims_ctx_kernel_ms(cosims_ctx *c, float *ms) {
+  if (!c || !ms) return fail(COSIMS_ERR_INVALID, "ctx and ms are required");
+  if (!c->timed) return fail(COSIMS_ERR_INVALID, "no trajectory kernel has run on this context");
+  DeviceGuard g(c->device);
+  cudaError_t e = cudaEventSynchronize(c->ev1);
+  if (e == cudaSuccess) e = cudaEventElapsedTime(ms, c->ev0, c->ev1);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel timing");
+  return COSIMS_OK;
 }
 
 cosims_status cosims_ctx_set_launch(cosims_ctx *c, int32_t group_lanes, int32_t block_threads) {

@@ -71,4 +71,6 @@ struct cosims_ctx {
   double *d_red = nullptr;
   int64_t red_cap = 0;
   cosims::LaunchShape last_shape{};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // around the last trajectory kernel
+  bool timed = false;
 };

@@ -63,6 +63,8 @@ def lib():
                 "cosims_batch_run": (st, [V, V, V, V, V, V]),
                 "cosims_batch_run_async": (st, [V, V, V, V, V, V]),
                 "cosims_batch_get_launch": (st, [V, C.c_int32, P(C.c_int32), P(C.c_int32)]),
+                "cosims_ctx_kernel_ms": (st, [V, P(C.c_float)]),
+                "cosims_probe_peaks": (st, [C.c_int32, P(C.c_double), P(C.c_double)]),
             }
             for name, (res, args) in sig.items():
                 f = getattr(L, name)
@@ -166,6 +168,12 @@ class Context:
         check(lib().cosims_run_sampled_device(self._h, seed, first, n, update_every,
                                               C.c_void_p(d_sums), _stream_ptr(stream)))
 
+    def kernel_ms(self) -> float:
+        """Device time of the last trajectory-kernel launch (CUDA events)."""
+        ms = C.c_float()
+        check(lib().cosims_ctx_kernel_ms(self._h, C.byref(ms)))
+        return ms.value
+
     def sample_inputs(self, seed: int, first: int, n: int, stream=None):
         ins = np.zeros(n, abi.TRAJ_IN_DTYPE)
         pos0, vel0 = np.zeros((n, 3)), np.zeros((n, 3))
@@ -173,6 +181,13 @@ class Context:
         check(lib().cosims_sample_inputs(self._h, seed, first, n, abi.vptr(ins), abi.vptr(pos0),
                                          abi.vptr(vel0), abi.vptr(hit), _stream_ptr(stream)))
         return ins, pos0, vel0, hit
+
+
+def probe_peaks(device: int = 0) -> tuple:
+    """Measured FP32 and FP64 FMA throughput of the device, TFLOP/s."""
+    f32, f64 = C.c_double(), C.c_double()
+    check(lib().cosims_probe_peaks(device, C.byref(f32), C.byref(f64)))
+    return f32.value, f64.value
 
 
 def omega(s: abi.CcsSums) -> tuple:

@@ -220,6 +220,17 @@ cosims_status cosims_sample_inputs(cosims_ctx *ctx, uint64_t seed, int64_t first
                                    int64_t n, cosims_traj_in *inputs, double *pos0,
                                    double *vel0, int32_t *hit, void *stream);
 
+/* Device time (ms) of this context's last trajectory-kernel launch, from CUDA
+ * events recorded around the launch on its stream; waits for the launch to
+ * finish.  No counterpart in the reference: it exists for measurement. */
+cosims_status cosims_ctx_kernel_ms(cosims_ctx *ctx, float *ms);
+
+/* Measured FMA throughput (TFLOP/s, FMA = 2 flops) of the FP32 and FP64
+ * vector pipes of `device`; either output may be NULL.  No counterpart in the
+ * reference: the roofline denominator for the trajectory kernels, which are
+ * bound by these pipes rather than by HBM or the tensor cores. */
+cosims_status cosims_probe_peaks(int32_t device, double *fp32_tflops, double *fp64_tflops);
+
 /* ---- batched: many molecules, one persistent launch -------------------- */
 typedef struct cosims_batch cosims_batch;
 
