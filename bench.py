@@ -201,6 +201,23 @@ def autotune(ctx, stream, torch, d_sums) -> int:
     return best
 
 
+def profile_case(args, mol, par, stream, torch) -> None:
+    """A small, self-contained run for profilers (one form, few launches)."""
+    from cosims_b200 import abi, engine
+    prec = abi.MIXED if args.profile == "mixed" else abi.PLAIN_F64
+    d_sums = torch.zeros(1024, dtype=torch.uint8, device="cuda")
+    with engine.Context(mol, par, prec) as ctx:
+        if args.group_lanes and prec == abi.MIXED:
+            ctx.set_launch(group_lanes=args.group_lanes)
+        n = args.profile_traj
+        for k in range(args.warmup + args.steps):
+            ctx.run_sampled_device(SEED, k * n, n, 0, d_sums.data_ptr(), stream)
+            ms = ctx.kernel_ms()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile": args.profile, "traj": n, "launch": ctx.get_launch(),
+                          "last_kernel_ms": ms}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -208,6 +225,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile", choices=["mixed", "plain"], default=None,
+                    help="small case for ncu: W + K integrals of --profile-traj trajectories "
+                         "of one form only, no L2 flush buffer, no sweep")
+    ap.add_argument("--profile-traj", type=int, default=20000)
+    ap.add_argument("--group-lanes", type=int, default=0)
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -233,6 +255,9 @@ def main():
     st = host.setup_from_files(mp, ip, seed=SEED)
     mol, par = st.mol, st.params
     stream = torch.cuda.current_stream()
+    if args.profile:
+        profile_case(args, mol, par, stream, torch)
+        return
     d_sums = torch.zeros(1024, dtype=torch.uint8, device="cuda")
     step_sums = torch.zeros((args.steps, 128), dtype=torch.uint8, device="cuda")
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
