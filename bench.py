@@ -392,7 +392,7 @@ def main():
                     "d2h_bytes_per_step": 24 * n_e2e,
                     "path": "cosims_run_list: pinned host start states -> device -> host "
                             "per-trajectory records"},
-            "gpu_launches": 4 * args.steps,
+            "gpu_launches": 7 * args.steps,   # sample, 3 x work order, trajectories, 2 x reduce
             "clocks": clk,
         }
         print(json.dumps(line))

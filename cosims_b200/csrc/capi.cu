@@ -2,6 +2,7 @@
 // launch sizing and the list / sampled run paths.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -126,16 +127,17 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   for (int k = 0; k < n; k++) perm[order[k]] = k;
 
   std::vector<AtomF64> a64(n);
-  std::vector<AtomF32> a32(n);
+  std::vector<float4> a4(n);
+  std::vector<float2> lj2(n);
+  std::vector<uint16_t> cid16(n);
   for (int k = 0; k < n; k++) {
     const int i = order[k];
     AtomF64 &A = a64[k];
     A.x = m->x[i]; A.y = m->y[i]; A.z = m->z[i]; A.q = m->charge[i];
     A.sig6 = m->sig6[i]; A.eps24m = m->eps24m[i]; A.eps4 = m->eps4[i];
-    AtomF32 &F = a32[k];
-    F.x = (float)A.x; F.y = (float)A.y; F.z = (float)A.z; F.q = (float)A.q;
-    F.sig6 = (float)A.sig6; F.eps24m = (float)A.eps24m;
-    F.cid = (uint32_t)cid[k]; F.pad = 0.f;
+    a4[k] = make_float4((float)A.x, (float)A.y, (float)A.z, (float)A.q);
+    lj2[k] = make_float2((float)A.sig6, (float)A.eps24m);
+    cid16[k] = (uint16_t)cid[k];
   }
   std::vector<ClusterF64> c64(nc);
   std::vector<ClusterF32> c32(nc);
@@ -183,7 +185,9 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   Builder b32;
   MolImage &i32 = h32.img;
   std::memset(&i32, 0, sizeof i32);
-  i32.off[S_ATOMS] = b32.add(a32.data(), sizeof(AtomF32) * n);
+  i32.off[S_ATOMS] = b32.add(a4.data(), sizeof(float4) * n);
+  i32.off[S_LJ] = b32.add(lj2.data(), sizeof(float2) * n);
+  i32.off[S_CID] = b32.add(cid16.data(), sizeof(uint16_t) * n);
   i32.off[S_CLUSTERS] = b32.add(c32.data(), sizeof(ClusterF32) * nc);
   b32.finish();
   i32.bytes = (uint32_t)b32.buf.size();
@@ -276,7 +280,16 @@ cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0
   LaunchShape ls;
   cosims_status st = launch_shape(c, n, ls);
   if (st != COSIMS_OK) return st;
+  if (n > INT32_MAX) return fail(COSIMS_ERR_UNSUPPORTED, "at most 2^31-1 trajectories per call");
   cudaStream_t s = (cudaStream_t)stream;
+  // longest-first work order (slow start speeds first)
+  st = grow(&c->d_order, &c->order_cap, n);
+  if (st == COSIMS_OK) st = grow(&c->d_order_scratch, &c->order_scratch_cap, order_scratch_len());
+  if (st != COSIMS_OK) return st;
+  if (n > 0) {
+    int orc = order_launch(c->par, d_vel0, d_hit, n, c->d_order, c->d_order_scratch, stream);
+    if (orc != 0) return cuda_fail((cudaError_t)orc, "work-order launch");
+  }
   cudaError_t e = cudaMemsetAsync(c->d_queue, 0, sizeof(unsigned long long), s);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * C_COUNT, s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
@@ -293,6 +306,7 @@ cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0
   a.pos0 = d_pos0;
   a.vel0 = d_vel0;
   a.hit = d_hit;
+  a.order = c->d_order;
   a.n = n;
   a.out = d_out;
   a.queue = c->d_queue;
@@ -414,6 +428,8 @@ void cosims_ctx_destroy(cosims_ctx *c) {
   cudaFree(c->d_vel0);
   cudaFree(c->d_red);
   cudaFree(c->d_hit);
+  cudaFree(c->d_order);
+  cudaFree(c->d_order_scratch);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   delete c;

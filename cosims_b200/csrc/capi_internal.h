@@ -70,6 +70,10 @@ struct cosims_ctx {
   int64_t hit_cap = 0;
   double *d_red = nullptr;
   int64_t red_cap = 0;
+  int32_t *d_order = nullptr;
+  int64_t order_cap = 0;
+  int32_t *d_order_scratch = nullptr;
+  int64_t order_scratch_cap = 0;
   cosims::LaunchShape last_shape{};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // around the last trajectory kernel
   bool timed = false;

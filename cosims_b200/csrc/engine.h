@@ -12,9 +12,11 @@
 //     reference's member order for the cluster force variants (1, 2, 3, 5),
 //     file order otherwise; perm[i] = force-order slot of file atom i
 //     (getPotential walks atoms in file order); ClusterF64 records.
-//   F32 image (mixed form): AtomF32 records in force order, ClusterF32
-//     records (FP64 centre and squared radii, so the near/far tests stay FP64;
-//     FP32 multipole moments).
+//   F32 image (mixed form): in force order, float4 (x, y, z, q), float2
+//     (sigma^6, 24 eps/mu) and uint16 cluster ids as separate arrays, so lanes
+//     reading consecutive atoms hit consecutive banks; ClusterF32 records (FP64
+//     centre and squared radii, so the near/far tests stay FP64; FP32
+//     multipole moments).
 #pragma once
 #include <cstdint>
 #include "cosims_cuda.h"
@@ -25,7 +27,7 @@ constexpr int kMaxAtoms = 16384;
 constexpr int kMaxClusters = 65535;
 constexpr int kMaxGroupLanes = 32;
 
-enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_COUNT };
+enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_LJ, S_CID, S_COUNT };
 
 struct AtomF64 {            // 56 bytes
   double x, y, z, q, sig6, eps24m, eps4;
@@ -44,13 +46,6 @@ struct ClusterF64 {         // 176 bytes
   int32_t pad;
 };
 
-struct AtomF32 {            // 32 bytes
-  float x, y, z, q;
-  float sig6, eps24m;
-  uint32_t cid;             // cluster of the atom (0 without clusters)
-  float pad;
-};
-
 struct ClusterF32 {         // 112 bytes
   double cx, cy, cz, mpr2, dr2;
   float q;
@@ -63,7 +58,6 @@ struct ClusterF32 {         // 112 bytes
 
 static_assert(sizeof(AtomF64) == 56, "AtomF64 layout");
 static_assert(sizeof(ClusterF64) == 176, "ClusterF64 layout");
-static_assert(sizeof(AtomF32) == 32, "AtomF32 layout");
 static_assert(sizeof(ClusterF32) == 112, "ClusterF32 layout");
 
 struct MolImage {
@@ -112,6 +106,7 @@ struct TrajArgs {
   const double *pos0;    // 3n start positions
   const double *vel0;    // 3n start velocities
   const int32_t *hit;    // n ellipsoid hits (NULL: every start state is a hit)
+  const int32_t *order;  // work order: queue slot -> trajectory (NULL: identity)
   int64_t n;
   cosims_traj_out *out;  // n records
   unsigned long long *queue;     // work counter (reset to 0 before launch)
@@ -125,6 +120,12 @@ int plain_max_smem_per_block();
 int sample_launch(const DevParams &par, uint64_t seed, int64_t first, int64_t n,
                   cosims_traj_in *inputs, double *pos0, double *vel0, int32_t *hit,
                   void *stream);
+// Longest-first work order: trajectories bucketed by start speed, slowest
+// first, misses last.  scratch: order_scratch_len() int32.
+constexpr int kOrderBuckets = 256;
+inline int64_t order_scratch_len() { return 2 * (kOrderBuckets + 1) + 8; }
+int order_launch(const DevParams &par, const double *vel0, const int32_t *hit, int64_t n,
+                 int32_t *order, int32_t *scratch, void *stream);
 
 // Reduction of per-trajectory records into a cosims_ccs_sums (device).
 int reduce_launch(const cosims_traj_out *recs, int64_t n, double ccs_const,

@@ -32,3 +32,74 @@ int sample_launch(const DevParams &par, uint64_t seed, int64_t first, int64_t n,
 }
 
 }  // namespace cosims
+
+namespace cosims {
+
+// ---- longest-first work order ---------------------------------------------------
+// Integration steps grow roughly as 1/g (the He crosses the ellipsoid at its
+// start speed), so handing out slow trajectories first keeps the last groups
+// of a launch from idling behind a few long trajectories.  A counting sort on
+// kOrderBuckets speed buckets, slowest first, misses last.  The order within
+// a bucket is not fixed (atomics), which does not matter: each trajectory's
+// result depends only on its own start state.
+
+__device__ __forceinline__ int speed_bucket(const DevParams &p, const double *vel0,
+                                            const int32_t *hit, int64_t i) {
+  if (hit && !hit[i]) return kOrderBuckets;   // misses last
+  const double vx = vel0[3 * i], vy = vel0[3 * i + 1], vz = vel0[3 * i + 2];
+  const double g = sqrt(vx * vx + vy * vy + vz * vz);
+  const double span = p.g_max - p.g_min;
+  int b = span > 0 ? (int)((g - p.g_min) / span * kOrderBuckets) : 0;
+  return b < 0 ? 0 : (b >= kOrderBuckets ? kOrderBuckets - 1 : b);
+}
+
+__global__ void order_hist(const DevParams p, const double *vel0, const int32_t *hit, int64_t n,
+                           int32_t *hist) {
+  __shared__ int32_t h[kOrderBuckets + 1];
+  for (int i = threadIdx.x; i <= kOrderBuckets; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&h[speed_bucket(p, vel0, hit, i)], 1);
+  __syncthreads();
+  for (int i = threadIdx.x; i <= kOrderBuckets; i += blockDim.x)
+    if (h[i]) atomicAdd(&hist[i], h[i]);
+}
+
+__global__ void order_scan(const int32_t *hist, int32_t *offset) {
+  if (threadIdx.x == 0) {
+    int32_t run = 0;
+    for (int i = 0; i <= kOrderBuckets; i++) {
+      offset[i] = run;
+      run += hist[i];
+    }
+  }
+}
+
+__global__ void order_scatter(const DevParams p, const double *vel0, const int32_t *hit,
+                              int64_t n, int32_t *offset, int32_t *order) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int b = speed_bucket(p, vel0, hit, i);
+    const int32_t slot = atomicAdd(&offset[b], 1);
+    order[slot] = (int32_t)i;
+  }
+}
+
+int order_launch(const DevParams &par, const double *vel0, const int32_t *hit, int64_t n,
+                 int32_t *order, int32_t *scratch, void *stream) {
+  if (n <= 0) return 0;
+  cudaStream_t s = (cudaStream_t)stream;
+  int32_t *hist = scratch, *offset = scratch + (kOrderBuckets + 1);
+  cudaError_t e = cudaMemsetAsync(hist, 0, sizeof(int32_t) * (kOrderBuckets + 1), s);
+  if (e != cudaSuccess) return (int)e;
+  const int block = 256;
+  int64_t grid = (n + block - 1) / block;
+  if (grid > 1184) grid = 1184;
+  order_hist<<<(unsigned)grid, block, 0, s>>>(par, vel0, hit, n, hist);
+  order_scan<<<1, 32, 0, s>>>(hist, offset);
+  order_scatter<<<(unsigned)grid, block, 0, s>>>(par, vel0, hit, n, offset, order);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace cosims

@@ -24,7 +24,9 @@ namespace mixed {
 enum ModeBits : uint8_t { M_ES = 1, M_LJ = 2, M_LJQ = 4 };
 
 struct View {
-  const AtomF32 *at;
+  const float4 *a4;        // x, y, z, q
+  const float2 *lj;        // sigma^6, 24 eps/mu
+  const uint16_t *cid;     // cluster of each atom
   const ClusterF32 *cl;
   int n, nc;
 };
@@ -36,7 +38,9 @@ struct View64 {   // FP64 image in global memory, for the energy check
 
 __device__ __forceinline__ View make_view(const unsigned char *b, const MolImage &img) {
   View v;
-  v.at = reinterpret_cast<const AtomF32 *>(b + img.off[S_ATOMS]);
+  v.a4 = reinterpret_cast<const float4 *>(b + img.off[S_ATOMS]);
+  v.lj = reinterpret_cast<const float2 *>(b + img.off[S_LJ]);
+  v.cid = reinterpret_cast<const uint16_t *>(b + img.off[S_CID]);
   v.cl = reinterpret_cast<const ClusterF32 *>(b + img.off[S_CLUSTERS]);
   v.n = img.n_atoms;
   v.nc = img.n_clusters;
@@ -62,6 +66,8 @@ struct Traits {
   static constexpr bool kClusters = TYPE == 1 || TYPE == 2 || TYPE == 3 || TYPE == 5;
   static constexpr bool kCharge = TYPE <= 4;
   static constexpr bool kFar = TYPE == 1 || TYPE == 2;
+  // every atom carries the charge field (types 3, 4): no per-pair branch
+  static constexpr bool kEsAlways = TYPE == 3 || TYPE == 4;
 };
 
 // Far-field monopole + dipole (+ quadrupole) terms of one cluster, in FP32,
@@ -116,24 +122,34 @@ __device__ __forceinline__ void far_terms(const View &m, int n, int order, float
   }
 }
 
-// One atom pair, FP32.  mode selects the field terms and which LJ parameters.
+// One atom pair, FP32.  mode selects the field terms and which LJ parameters;
+// mode 0 (an idle lane or an atom outside every cut-off) contributes nothing.
+// The LJ term is branch-free (a zero prefactor switches it off), so two calls
+// in a row interleave; the field terms branch only for the multipole variants.
 template <int TYPE>
 __device__ __forceinline__ void pair(const View &m, int k, uint32_t mode, float hx, float hy,
                                      float hz, float lx, float ly, float lz, Acc &s) {
-  const AtomF32 a = m.at[k];
-  const float dx = (hx - a.x) + lx, dy = (hy - a.y) + ly, dz = (hz - a.z) + lz;
+  const bool act = mode != 0u;
+  const int kk = act ? k : 0;
+  const float4 a = m.a4[kk];
+  float2 lj = m.lj[kk];
+  if (TYPE == 1 && (mode & M_LJQ)) {
+    const ClusterF32 &C = m.cl[m.cid[kk]];
+    lj = make_float2(C.qsig6, C.qeps);
+  }
+  const float eps = (mode & (M_LJ | M_LJQ)) ? lj.y : 0.0f;
+  const float dx = act ? (hx - a.x) + lx : 1.0e3f;
+  const float dy = act ? (hy - a.y) + ly : 1.0e3f;
+  const float dz = act ? (hz - a.z) + lz : 1.0e3f;
   const float r2 = dx * dx + dy * dy + dz * dz;
   const float ir = rsqrtf(r2);
   const float ir2 = ir * ir;
-  if (mode & (M_LJ | M_LJQ)) {
-    float sig6 = a.sig6, eps = a.eps24m;
-    if (TYPE == 1 && (mode & M_LJQ)) { sig6 = m.cl[a.cid].qsig6; eps = m.cl[a.cid].qeps; }
-    const float s6 = sig6 * (ir2 * ir2 * ir2);
-    const float f = eps * ir2 * s6 * (2.0f * s6 - 1.0f);
-    s.Fx += f * dx; s.Fy += f * dy; s.Fz += f * dz;
-  }
-  if (Traits<TYPE>::kCharge && (mode & M_ES)) {
-    const float q3 = a.q * ir * ir2;
+  const float s6 = lj.x * (ir2 * ir2 * ir2);
+  const float f = eps * ir2 * s6 * (2.0f * s6 - 1.0f);
+  s.Fx += f * dx; s.Fy += f * dy; s.Fz += f * dz;
+  if (Traits<TYPE>::kCharge && (Traits<TYPE>::kEsAlways || (mode & M_ES))) {
+    const float q = (Traits<TYPE>::kEsAlways && !(mode & M_ES)) ? 0.0f : a.w;
+    const float q3 = q * ir * ir2;
     const float q5 = q3 * ir2;
     s.Ex += q3 * dx; s.Ey += q3 * dy; s.Ez += q3 * dz;
     s.Q3 += q3;
@@ -177,19 +193,25 @@ __device__ void force(const View &m, const DevParams &p, const double pos[3], do
       modes[c] = mode;
     }
     __syncwarp();
-    // pass 2: atoms, G at a time; the trip count is the same for every lane
-    for (int base = 0; base < m.n; base += G) {
-      const int k = base + lane;
-      const uint32_t mode = k < m.n ? modes[m.at[k].cid] : 0u;
-      if (mode) {
-        pair<TYPE>(m, k, mode, hx, hy, hz, lx, ly, lz, s);
-        if (mode & M_ES) w.es++; else w.lj++;
-      }
+    // pass 2: atoms, 2G at a time (two independent pairs per lane); the trip
+    // count is the same for every lane of the warp
+    for (int base = 0; base < m.n; base += 2 * G) {
+      const int k0 = base + lane, k1 = k0 + G;
+      const uint32_t m0 = k0 < m.n ? modes[m.cid[k0]] : 0u;
+      const uint32_t m1 = k1 < m.n ? modes[m.cid[k1]] : 0u;
+      pair<TYPE>(m, k0, m0, hx, hy, hz, lx, ly, lz, s);
+      pair<TYPE>(m, k1, m1, hx, hy, hz, lx, ly, lz, s);
+      w.es += ((m0 & M_ES) != 0) + ((m1 & M_ES) != 0);
+      w.lj += (m0 && !(m0 & M_ES)) + (m1 && !(m1 & M_ES));
     }
     __syncwarp();
   } else {
     constexpr uint32_t mode = TYPE == 4 ? (M_ES | M_LJ) : M_LJ;
-    for (int k = lane; k < m.n; k += G) pair<TYPE>(m, k, mode, hx, hy, hz, lx, ly, lz, s);
+    for (int base = 0; base < m.n; base += 2 * G) {
+      const int k0 = base + lane, k1 = k0 + G;
+      pair<TYPE>(m, k0, k0 < m.n ? mode : 0u, hx, hy, hz, lx, ly, lz, s);
+      pair<TYPE>(m, k1, k1 < m.n ? mode : 0u, hx, hy, hz, lx, ly, lz, s);
+    }
     const uint32_t mine = lane < m.n ? (uint32_t)((m.n - 1 - lane) / G + 1) : 0u;
     if (TYPE == 4) w.es += mine; else w.lj += mine;
   }
@@ -311,6 +333,7 @@ __global__ void __launch_bounds__(256) traj_mixed_kernel(const TrajArgs a) {
         if (lane == 0) tk = (long long)atomicAdd(a.queue, 1ull);
         t = __shfl_sync(gmask, tk, 0, G);
         if (t >= a.n) { phase = P_DONE; break; }
+        if (a.order) t = a.order[t];
         if (a.hit && !a.hit[t]) {                 // ellipsoid miss: chi = 0
           if (lane == 0) {
             cosims_traj_out o = {0.0, 0.0, 0, 0u};

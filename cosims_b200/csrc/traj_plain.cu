@@ -394,6 +394,7 @@ __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
       for (;;) {
         t = (long long)atomicAdd(a.queue, 1ull);
         if (t >= a.n) { phase = P_DONE; break; }
+        if (a.order) t = a.order[t];
         if (a.hit && !a.hit[t]) {                 // ellipsoid miss: chi = 0
           cosims_traj_out o = {0.0, 0.0, 0, 0u};
           a.out[t] = o;
