@@ -231,6 +231,29 @@ cosims_status cosims_ctx_kernel_ms(cosims_ctx *ctx, float *ms);
  * bound by these pipes rather than by HBM or the tensor cores. */
 cosims_status cosims_probe_peaks(int32_t device, double *fp32_tflops, double *fp64_tflops);
 
+/* ---- no device allocation ------------------------------------------------ */
+/* No counterpart in the reference.  For callers that cannot let this library
+ * allocate device memory -- a host program that owns the GPU's memory through
+ * its own pool or arena, or one that forbids cudaMalloc (which synchronises
+ * the device and can fail mid-run) on its hot path.  It runs the list form
+ * (as cosims_run_list_device) without a context and allocates nothing: the
+ * caller passes the molecule and scalars (host), device buffers d_pos0 /
+ * d_vel0 (3n doubles each) and d_out (n records); the molecule image, work
+ * queue, work order and counters live in one static 8 MiB device array that
+ * every GPU loading this library holds until the process exits.  Limits: at
+ * most 1,571,840 trajectories per call and a molecule image of at most 2 MiB
+ * (every molecule within the 16384-atom limit fits); larger requests return
+ * COSIMS_ERR_UNSUPPORTED before any device work.  The first call on a device
+ * looks up its array (cudaGetSymbolAddress, with that device current) and
+ * should come before any stream capture.  Calls share the array: calls that
+ * overlap on the GPU (other streams or host threads) race; run them in turn.
+ * Stream-ordered: returns without synchronising.  group_lanes: lanes per
+ * trajectory of the mixed form (ignored by the plain form). */
+cosims_status cosims_run_list_noalloc(const cosims_molecule *mol, const cosims_params *par,
+                                      int32_t precision, int32_t group_lanes,
+                                      const double *d_pos0, const double *d_vel0, int64_t n,
+                                      cosims_traj_out *d_out, void *stream);
+
 /* ---- batched: many molecules, one persistent launch -------------------- */
 typedef struct cosims_batch cosims_batch;
 
