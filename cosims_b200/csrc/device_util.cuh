@@ -68,16 +68,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 // 2^20 - 1 bytes: the mbarrier transaction-count range) from global to shared
 // memory.  Call from all threads of the CTA.  Returns false, in every thread,
 // when a bounded wait gave up (the caller flags an error and returns).
+// `init`: the first staging through this barrier (initialises it); later
+// stagings pass init = false and the parity of their phase (0, 1, 0, ...).
 __device__ __forceinline__ bool stage_to_smem(void *dst, const void *src, uint32_t bytes,
-                                              uint64_t *bar, uint32_t parity) {
-  if (threadIdx.x == 0) {
-    if (parity == 0) {
-      mbar_init(bar, 1);
-      fence_barrier_init();
-    }
+                                              uint64_t *bar, uint32_t parity, bool init) {
+  if (threadIdx.x == 0 && init) {
+    mbar_init(bar, 1);
+    fence_barrier_init();
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    // order earlier generic-proxy reads/writes of this shared memory before
+    // the async-proxy writes of the bulk copies
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     mbar_arrive_expect_tx(bar, bytes);
     for (uint32_t o = 0; o < bytes; o += kBulkChunk) {
       uint32_t n = bytes - o < kBulkChunk ? bytes - o : kBulkChunk;

@@ -113,6 +113,50 @@ struct TrajArgs {
   unsigned long long *counters;  // C_COUNT counters
 };
 
+// ---- batched form ---------------------------------------------------------------
+// One molecule of a batch (device-resident; copied to shared memory per item).
+struct BatchMol {
+  MolImage img32;        // F32 image in the batch arena
+  MolImage img64;        // F64 image in the batch arena (energy check)
+  DevParams par;
+  int32_t type;          // force variant
+  int32_t group_lanes;   // lanes per trajectory
+  int32_t mode_stride;   // bytes of cluster-mode scratch per group
+  int32_t use_smem;      // stage the F32 image in shared memory
+  int64_t base;          // first slot of this molecule in the batch arrays
+  int64_t n_traj;        // trajectories this run
+  uint64_t seed;         // Philox key
+  int64_t first_index;   // first trajectory index of the stream
+};
+
+// A work item: trajectories [t0, t1) of one molecule (molecule-local indices).
+struct BatchItem {
+  int32_t mol, pad;
+  int64_t t0, t1;
+};
+
+struct BatchArgs {
+  const BatchMol *mols;
+  const BatchItem *items;
+  int32_t n_items;
+  int32_t n_mols;
+  uint32_t smem_bytes;   // dynamic shared memory of the launch
+  uint32_t pad;
+  const double *pos0;    // batch-wide start states (3 per slot)
+  const double *vel0;
+  const int32_t *hit;
+  cosims_traj_out *out;  // batch-wide records
+  unsigned long long *item_queue;
+  unsigned long long *counters;
+};
+
+int batch_launch(const BatchArgs &a, int block, int grid, size_t smem, void *stream);
+int batch_occupancy(int block, size_t smem, int *per_sm);
+int batch_sample_launch(const BatchMol *mols, int n_mols, int64_t total, double *pos0,
+                        double *vel0, int32_t *hit, void *stream);
+int batch_reduce_launch(const BatchMol *mols, int n_mols, const cosims_traj_out *recs,
+                        int64_t update_every, cosims_ccs_sums *sums, void *stream);
+
 // Host helpers implemented in the .cu files.
 int plain_launch(const TrajArgs &a, int block, int grid, size_t smem, void *stream);
 int mixed_launch(const TrajArgs &a, int block, int grid, size_t smem, void *stream);

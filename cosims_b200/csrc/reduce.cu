@@ -173,3 +173,91 @@ int reduce_launch(const cosims_traj_out *recs, int64_t n, double ccs_const, int 
 }
 
 }  // namespace cosims
+
+namespace cosims {
+
+// ---- batched reduction: one CTA per molecule ------------------------------------------
+// The same fixed-order sums and one-thread n_eff bookkeeping as reduce_final,
+// over each molecule's records [base, base + n_traj).  Contributions use
+// 2 sin^2(chi/2) (the batched form is the mixed form).  Work counters are
+// reported for the whole batch by cosims_batch_counters, so they are 0 here.
+__global__ void batch_reduce_kernel(const BatchMol *mols, const cosims_traj_out *__restrict__ recs,
+                                    long long update_every, cosims_ccs_sums *sums) {
+  __shared__ double s_sum[kFinalThreads], s_sum2[kFinalThreads], s_max[kFinalThreads];
+  __shared__ long long s_hit[kFinalThreads], s_succ[kFinalThreads];
+  __shared__ long long s_f0[kFinalThreads], s_f1[kFinalThreads];
+  __shared__ int s_e0[kFinalThreads], s_e1[kFinalThreads];
+  const BatchMol &bm = mols[blockIdx.x];
+  const cosims_traj_out *r = recs + bm.base;
+  const long long n = bm.n_traj;
+  const double c = bm.par.ccs_const;
+  const int t = threadIdx.x;
+  const long long chunk = (n + kFinalThreads - 1) / kFinalThreads;
+  double sum = 0, sum2 = 0, mx = 0;
+  long long hit = 0, succ = 0;
+  for (long long i = (long long)t * chunk; i < n && i < (long long)(t + 1) * chunk; i++) {
+    const cosims_traj_out x = r[i];
+    const double v = contribution(x, c, 1);
+    sum += v;
+    sum2 += v * v;
+    if (x.status & COSIMS_TRAJ_HIT) {
+      hit++;
+      if (x.status & COSIMS_TRAJ_SUCCESS) { succ++; mx = fmax(mx, x.de_pct); }
+    }
+  }
+  s_sum[t] = sum; s_sum2[t] = sum2; s_max[t] = mx; s_hit[t] = hit; s_succ[t] = succ;
+  long long w0 = 0;
+  if (update_every > 0) w0 = n - n % update_every;
+  const long long wl = n - w0;
+  const long long seg = (wl + kFinalThreads - 1) / kFinalThreads;
+  const long long s0 = w0 + (long long)t * seg, s1 = min(n, s0 + seg);
+  int e0 = 0, e1 = 1;
+  long long f0 = 0, f1 = 0;
+  for (long long i = s0; i < s1; i++) {
+    const cosims_traj_out x = r[i];
+    e0 = eff_of(x, e0);
+    e1 = eff_of(x, e1);
+    f0 += !e0;
+    f1 += !e1;
+  }
+  s_f0[t] = f0; s_f1[t] = f1; s_e0[t] = e0; s_e1[t] = e1;
+  __syncthreads();
+  for (int o = kFinalThreads / 2; o > 0; o >>= 1) {
+    if (t < o) {
+      s_sum[t] += s_sum[t + o];
+      s_sum2[t] += s_sum2[t + o];
+      s_max[t] = fmax(s_max[t], s_max[t + o]);
+      s_hit[t] += s_hit[t + o];
+      s_succ[t] += s_succ[t + o];
+    }
+    __syncthreads();
+  }
+  if (t == 0) {
+    int carried = 0;
+    for (long long i = w0 - 1; i >= 0; i--) {
+      const cosims_traj_out x = r[i];
+      if (x.status & COSIMS_TRAJ_HIT) { carried = (x.status & COSIMS_TRAJ_SUCCESS) ? 1 : 0; break; }
+    }
+    long long fails = 0;
+    for (int k = 0; k < kFinalThreads; k++) {
+      if (w0 + (long long)k * seg >= n) break;
+      fails += carried ? s_f1[k] : s_f0[k];
+      carried = carried ? s_e1[k] : s_e0[k];
+    }
+    cosims_ccs_sums s;
+    memset(&s, 0, sizeof s);
+    s.sum = s_sum[0]; s.sum2 = s_sum2[0]; s.max_de_pct = s_max[0];
+    s.n = n; s.n_hit = s_hit[0]; s.n_success = s_succ[0]; s.n_eff = n - fails;
+    sums[blockIdx.x] = s;
+  }
+}
+
+int batch_reduce_launch(const BatchMol *mols, int n_mols, const cosims_traj_out *recs,
+                        int64_t update_every, cosims_ccs_sums *sums, void *stream) {
+  if (n_mols <= 0) return 0;
+  batch_reduce_kernel<<<n_mols, kFinalThreads, 0, (cudaStream_t)stream>>>(mols, recs, update_every,
+                                                                          sums);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace cosims

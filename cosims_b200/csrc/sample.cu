@@ -103,3 +103,42 @@ int order_launch(const DevParams &par, const double *vel0, const int32_t *hit, i
 }
 
 }  // namespace cosims
+
+namespace cosims {
+
+// ---- batched sampling ---------------------------------------------------------------
+// Slot i of the batch belongs to the molecule whose [base, base + n_traj)
+// holds it (molecules sorted by base); its start values are those of
+// trajectory first_index + (i - base) of that molecule's stream, exactly as
+// the single-molecule sampler draws them.
+__global__ void batch_sample_kernel(const BatchMol *mols, int n_mols, int64_t total, double *pos0,
+                                    double *vel0, int32_t *hit) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = n_mols - 1;
+    while (lo < hi) {                       // last molecule with base <= i
+      const int mid = (lo + hi + 1) >> 1;
+      if (mols[mid].base <= i) lo = mid; else hi = mid - 1;
+    }
+    const BatchMol &bm = mols[lo];
+    const int64_t t = i - bm.base;
+    double ps[3] = {0, 0, 0}, vs[3] = {0, 0, 0};
+    bool h = false;
+    if (t < bm.n_traj) {
+      cosims_traj_in in = sample_inputs(bm.par, bm.seed, (uint64_t)(bm.first_index + t));
+      h = start_state(bm.par, in, ps, vs);
+    }
+    for (int k = 0; k < 3; k++) { pos0[3 * i + k] = ps[k]; vel0[3 * i + k] = vs[k]; }
+    hit[i] = h ? 1 : 0;
+  }
+}
+
+int batch_sample_launch(const BatchMol *mols, int n_mols, int64_t total, double *pos0,
+                        double *vel0, int32_t *hit, void *stream) {
+  if (total <= 0 || n_mols <= 0) return 0;
+  batch_sample_kernel<<<1184, 256, 0, (cudaStream_t)stream>>>(mols, n_mols, total, pos0, vel0,
+                                                              hit);
+  return (int)cudaGetLastError();
+}
+
+}  // namespace cosims

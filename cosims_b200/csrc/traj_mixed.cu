@@ -282,27 +282,42 @@ __device__ __forceinline__ double angle3(const double a[3], const double b[3]) {
 
 enum Phase : int { P_ACQUIRE = 0, P_INIT_FIRST, P_INIT_RETRY, P_STEP, P_DONE };
 
+// Work counters of one thread, flushed to the device counters at kernel end.
+struct Tally {
+  uint32_t lj = 0, es = 0, far = 0, nforce = 0, npot = 0, npotpairs = 0;
+  unsigned long long nsteps = 0;
+};
+
+// Pair counters are per lane; step and evaluation counters are kept by each
+// group's lane 0 only, so a plain sum over threads is right for any G.
+__device__ __forceinline__ void flush_tally(const Tally &tl, unsigned long long *c) {
+  count_add(c, C_PAIR_LJ, tl.lj);
+  count_add(c, C_PAIR_ES, tl.es);
+  count_add(c, C_FAR, tl.far);
+  count_add(c, C_STEPS, (long long)tl.nsteps);
+  count_add(c, C_FORCE_EVALS, tl.nforce);
+  count_add(c, C_POT_EVALS, tl.npot);
+  count_add(c, C_PAIR_POT, tl.npotpairs);
+}
+
+// The trajectory loop of one group of G lanes (every warp of the CTA calls it
+// together).  Groups take queue slots 0..n-1 from `queue` (global or shared
+// memory); slot k integrates trajectory order[k] (k without an order), whose
+// start state is pos0/vel0[3t..3t+2] and whose record goes to out[t]; a
+// trajectory with hit[t] == 0 is an ellipsoid miss.  Every iteration
+// evaluates one acceleration per group (at the start state or after a
+// position update) and, when any group of the warp needs it, one potential;
+// a group whose trajectory ends takes the next slot at once.
 template <int TYPE>
-__global__ void __launch_bounds__(256) traj_mixed_kernel(const TrajArgs a) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ uint64_t bar;
-  const unsigned char *base = a.img.gbase;
-  if (a.use_smem) {
-    if (!stage_to_smem(smem, a.img.gbase, a.img.bytes, &bar, 0)) {
-      if (threadIdx.x == 0) atomicOr(a.counters + C_ERROR, 1ull);
-      return;
-    }
-    base = smem;
-  }
-  const View m = make_view(base, a.img);
-  const View64 m64 = make_view64(a.img64);
-  const DevParams &p = a.par;
-  const int G = a.group_lanes;
+__device__ __forceinline__ void group_loop(const View &m, const View64 &m64, const DevParams &p,
+                                           int G, uint8_t *modes, const double *pos0,
+                                           const double *vel0, const int32_t *hit,
+                                           const int32_t *order, long long n,
+                                           cosims_traj_out *out, unsigned long long *queue,
+                                           Tally &tl) {
   const int lane = threadIdx.x & (G - 1);
-  const int group = threadIdx.x / G;
   const unsigned gmask = G == 32 ? 0xffffffffu
                                  : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
-  uint8_t *modes = smem + (a.use_smem ? a.img.bytes : 0) + (size_t)group * a.mode_stride;
   const long long cap = p.max_steps > 0 ? p.max_steps : kDefaultMaxSteps;
 
   double p0[3] = {0, 0, 0}, v0[3] = {0, 0, 0}, pos[3] = {0, 0, 0}, vel[3] = {0, 0, 0},
@@ -311,9 +326,6 @@ __global__ void __launch_bounds__(256) traj_mixed_kernel(const TrajArgs a) {
   int orbits = 0, step = 0, phase = P_ACQUIRE;
   long long total = 0, t = 0;
   unsigned etries = 0, otries = 0;
-  WorkM w = {0, 0, 0};
-  uint32_t nforce = 0, npot = 0, npotpairs = 0;
-  unsigned long long nsteps = 0;
 
   auto finish = [&](double chi, double de, int steps, uint32_t status) {
     if (lane == 0) {
@@ -321,7 +333,7 @@ __global__ void __launch_bounds__(256) traj_mixed_kernel(const TrajArgs a) {
       o.chi = chi; o.de_pct = de; o.steps = steps;
       o.status = status | (etries << COSIMS_TRAJ_ETRIES_SHIFT) |
                  (otries << COSIMS_TRAJ_OTRIES_SHIFT);
-      a.out[t] = o;
+      out[t] = o;
     }
     phase = P_ACQUIRE;
   };
@@ -330,18 +342,18 @@ __global__ void __launch_bounds__(256) traj_mixed_kernel(const TrajArgs a) {
     if (phase == P_ACQUIRE) {
       for (;;) {
         long long tk = 0;
-        if (lane == 0) tk = (long long)atomicAdd(a.queue, 1ull);
+        if (lane == 0) tk = (long long)atomicAdd(queue, 1ull);
         t = __shfl_sync(gmask, tk, 0, G);
-        if (t >= a.n) { phase = P_DONE; break; }
-        if (a.order) t = a.order[t];
-        if (a.hit && !a.hit[t]) {                 // ellipsoid miss: chi = 0
+        if (t >= n) { phase = P_DONE; break; }
+        if (order) t = order[t];
+        if (hit && !hit[t]) {                 // ellipsoid miss: chi = 0
           if (lane == 0) {
             cosims_traj_out o = {0.0, 0.0, 0, 0u};
-            a.out[t] = o;
+            out[t] = o;
           }
           continue;
         }
-        for (int i = 0; i < 3; i++) { p0[i] = a.pos0[3 * t + i]; v0[i] = a.vel0[3 * t + i]; }
+        for (int i = 0; i < 3; i++) { p0[i] = pos0[3 * t + i]; v0[i] = vel0[3 * t + i]; }
         phase = P_INIT_FIRST;
         break;
       }
@@ -376,9 +388,10 @@ __global__ void __launch_bounds__(256) traj_mixed_kernel(const TrajArgs a) {
     double U = 0;
     if (__any_sync(0xffffffffu, needU)) U = potential(m64, p, ep, G, lane);
     if (phase == P_DONE) continue;
-    nforce++;
-    w.lj += wi.lj; w.es += wi.es; w.far += wi.far;
-    if (needU) { npot++; npotpairs += (uint32_t)m64.n; }
+    const uint32_t lead = lane == 0 ? 1u : 0u;
+    tl.nforce += lead;
+    tl.lj += wi.lj; tl.es += wi.es; tl.far += wi.far;
+    if (needU) { tl.npot += lead; tl.npotpairs += lead * (uint32_t)m64.n; }
 
     if (phase == P_INIT_FIRST || phase == P_INIT_RETRY) {
       if (phase == P_INIT_FIRST) E0 = U + 0.5 * p.mu * dot3(v0, v0);
@@ -392,7 +405,7 @@ __global__ void __launch_bounds__(256) traj_mixed_kernel(const TrajArgs a) {
     for (int i = 0; i < 3; i++) { vel[i] = vel[i] + an[i] * dt * 0.5; acc[i] = an[i]; }
     step++;
     total++;
-    nsteps++;
+    tl.nsteps += lead;
     bool track = true;
     const double rold = rdot;
     rdot = dot3(pos, vel);
@@ -426,16 +439,97 @@ __global__ void __launch_bounds__(256) traj_mixed_kernel(const TrajArgs a) {
       else if (step == 0) phase = P_INIT_RETRY;
     }
   }
-  unsigned long long *c = a.counters;
-  count_add(c, C_PAIR_LJ, w.lj);
-  count_add(c, C_PAIR_ES, w.es);
-  count_add(c, C_FAR, w.far);
-  if (lane == 0) {
-    count_add(c, C_STEPS, (long long)nsteps);
-    count_add(c, C_FORCE_EVALS, nforce);
-    count_add(c, C_POT_EVALS, npot);
-    count_add(c, C_PAIR_POT, npotpairs);
+}
+
+template <int TYPE>
+__global__ void __launch_bounds__(256) traj_mixed_kernel(const TrajArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar;
+  const unsigned char *base = a.img.gbase;
+  if (a.use_smem) {
+    if (!stage_to_smem(smem, a.img.gbase, a.img.bytes, &bar, 0, true)) {
+      if (threadIdx.x == 0) atomicOr(a.counters + C_ERROR, 1ull);
+      return;
+    }
+    base = smem;
   }
+  const View m = make_view(base, a.img);
+  const View64 m64 = make_view64(a.img64);
+  const int G = a.group_lanes;
+  uint8_t *modes =
+      smem + (a.use_smem ? a.img.bytes : 0) + (size_t)(threadIdx.x / G) * a.mode_stride;
+  Tally tl;
+  group_loop<TYPE>(m, m64, a.par, G, modes, a.pos0, a.vel0, a.hit, a.order, a.n, a.out,
+                   a.queue, tl);
+  flush_tally(tl, a.counters);
+}
+
+// ---- batched form: one persistent launch over many molecules ------------------
+// CTAs take work items (a molecule and a range of its trajectories) from a
+// device queue.  When an item's molecule differs from the one staged, the CTA
+// waits for its groups, then bulk-copies the new image into shared memory
+// (molecules over the launch's shared-memory budget are read through L1/L2).
+// Groups then take the item's trajectories from a shared-memory counter.
+template <int TYPE>
+__device__ __forceinline__ void batch_item(const BatchMol &bm, const unsigned char *base,
+                                           uint8_t *modes_base, const BatchArgs &a,
+                                           const BatchItem &it, unsigned long long *q,
+                                           Tally &tl) {
+  const View m = make_view(base, bm.img32);
+  const View64 m64 = make_view64(bm.img64);
+  const int G = bm.group_lanes;
+  uint8_t *modes = modes_base + (size_t)(threadIdx.x / G) * bm.mode_stride;
+  const long long b = bm.base + it.t0;
+  group_loop<TYPE>(m, m64, bm.par, G, modes, a.pos0 + 3 * b, a.vel0 + 3 * b, a.hit + b,
+                   nullptr, it.t1 - it.t0, a.out + b, q, tl);
+}
+
+__global__ void __launch_bounds__(256) batch_mixed_kernel(const BatchArgs a) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  __shared__ uint64_t bar;
+  __shared__ BatchMol cur;
+  __shared__ int s_item, s_mol;
+  __shared__ unsigned long long s_queue;
+  if (threadIdx.x == 0) s_mol = -1;
+  uint32_t stagings = 0;
+  Tally tl;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = (int)atomicAdd(a.item_queue, 1ull);
+    __syncthreads();
+    const int item = s_item;
+    if (item >= a.n_items) break;
+    const BatchItem it = a.items[item];
+    if (it.mol != s_mol) {
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        cur = a.mols[it.mol];
+        s_mol = it.mol;
+      }
+      __syncthreads();
+      if (cur.use_smem) {
+        if (!stage_to_smem(smem, cur.img32.gbase, cur.img32.bytes, &bar, stagings & 1u,
+                           stagings == 0)) {
+          if (threadIdx.x == 0) atomicOr(a.counters + C_ERROR, 1ull);
+          return;
+        }
+        stagings++;
+      }
+    }
+    if (threadIdx.x == 0) s_queue = 0ull;
+    __syncthreads();
+    const unsigned char *base = cur.use_smem ? smem : cur.img32.gbase;
+    uint8_t *modes = smem + (cur.use_smem ? cur.img32.bytes : 0);
+    switch (cur.type) {
+      case 1: batch_item<1>(cur, base, modes, a, it, &s_queue, tl); break;
+      case 2: batch_item<2>(cur, base, modes, a, it, &s_queue, tl); break;
+      case 3: batch_item<3>(cur, base, modes, a, it, &s_queue, tl); break;
+      case 4: batch_item<4>(cur, base, modes, a, it, &s_queue, tl); break;
+      case 5: batch_item<5>(cur, base, modes, a, it, &s_queue, tl); break;
+      default: batch_item<6>(cur, base, modes, a, it, &s_queue, tl); break;
+    }
+    __syncthreads();   // every group is done with the item before a restage
+  }
+  flush_tally(tl, a.counters);
 }
 
 template <int TYPE>
@@ -450,6 +544,26 @@ int launch_t(const TrajArgs &a, int block, int grid, size_t smem, void *stream) 
 }
 
 }  // namespace mixed
+
+int batch_launch(const BatchArgs &a, int block, int grid, size_t smem, void *stream) {
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(mixed::batch_mixed_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+  }
+  mixed::batch_mixed_kernel<<<grid, block, smem, (cudaStream_t)stream>>>(a);
+  return (int)cudaGetLastError();
+}
+
+int batch_occupancy(int block, size_t smem, int *per_sm) {
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(mixed::batch_mixed_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return (int)e;
+  }
+  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, mixed::batch_mixed_kernel,
+                                                            block, smem);
+}
 
 int mixed_launch(const TrajArgs &a, int block, int grid, size_t smem, void *stream) {
   switch (a.par.force_type) {

@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
   __shared__ uint64_t bar;
   const unsigned char *base = a.img.gbase;
   if (a.use_smem) {
-    if (!stage_to_smem(smem, a.img.gbase, a.img.bytes, &bar, 0)) {
+    if (!stage_to_smem(smem, a.img.gbase, a.img.bytes, &bar, 0, true)) {
       if (threadIdx.x == 0) atomicOr(a.counters + C_ERROR, 1ull);
       return;
     }

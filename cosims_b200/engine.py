@@ -63,6 +63,8 @@ def lib():
                 "cosims_batch_run": (st, [V, V, V, V, V, V]),
                 "cosims_batch_run_async": (st, [V, V, V, V, V, V]),
                 "cosims_batch_get_launch": (st, [V, C.c_int32, P(C.c_int32), P(C.c_int32)]),
+                "cosims_batch_set_update_every": (st, [V, C.c_int64]),
+                "cosims_batch_counters": (st, [V, P(abi.CcsSums), P(C.c_float)]),
                 "cosims_ctx_kernel_ms": (st, [V, P(C.c_float)]),
                 "cosims_probe_peaks": (st, [C.c_int32, P(C.c_double), P(C.c_double)]),
             }
@@ -181,6 +183,72 @@ class Context:
         check(lib().cosims_sample_inputs(self._h, seed, first, n, abi.vptr(ins), abi.vptr(pos0),
                                          abi.vptr(vel0), abi.vptr(hit), _stream_ptr(stream)))
         return ins, pos0, vel0, hit
+
+
+class Batch:
+    """Many molecules in one persistent launch (mixed precision)."""
+
+    def __init__(self, mols: list, pars: list, device: int = 0):
+        self.mols = mols
+        self.pars = pars
+        self.device = device
+        self._views = (abi.Molecule * len(mols))(*[m.view() for m in mols])
+        self._pars = (abi.Params * len(pars))(*pars)
+        h = C.c_void_p()
+        check(lib().cosims_batch_create(C.cast(self._views, C.c_void_p),
+                                        C.cast(self._pars, C.c_void_p), len(mols), abi.MIXED,
+                                        device, C.byref(h)))
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            lib().cosims_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def autotune(self, stream=None) -> None:
+        check(lib().cosims_batch_autotune(self._h, _stream_ptr(stream)))
+
+    def launch(self, mol: int) -> tuple:
+        g, it = C.c_int32(), C.c_int32()
+        check(lib().cosims_batch_get_launch(self._h, mol, C.byref(g), C.byref(it)))
+        return g.value, it.value
+
+    def set_update_every(self, k: int) -> None:
+        check(lib().cosims_batch_set_update_every(self._h, int(k)))
+
+    def run(self, seeds, firsts, n_traj, stream=None) -> list:
+        k = len(self.mols)
+        sd = np.ascontiguousarray(seeds, dtype=np.uint64)
+        fi = np.ascontiguousarray(firsts, dtype=np.int64)
+        nt = np.ascontiguousarray(n_traj, dtype=np.int64)
+        out = (abi.CcsSums * k)()
+        check(lib().cosims_batch_run(self._h, abi.vptr(sd), abi.vptr(fi), abi.vptr(nt),
+                                     C.cast(out, C.c_void_p), _stream_ptr(stream)))
+        return list(out)
+
+    def run_async(self, seeds, firsts, n_traj, d_sums: int = 0, stream=None) -> None:
+        sd = np.ascontiguousarray(seeds, dtype=np.uint64)
+        fi = np.ascontiguousarray(firsts, dtype=np.int64)
+        nt = np.ascontiguousarray(n_traj, dtype=np.int64)
+        check(lib().cosims_batch_run_async(self._h, abi.vptr(sd), abi.vptr(fi), abi.vptr(nt),
+                                           C.c_void_p(d_sums), _stream_ptr(stream)))
+
+    def counters(self) -> tuple:
+        w, ms = abi.CcsSums(), C.c_float()
+        check(lib().cosims_batch_counters(self._h, C.byref(w), C.byref(ms)))
+        return w, ms.value
 
 
 def probe_peaks(device: int = 0) -> tuple:

@@ -280,6 +280,13 @@ cosims_status cosims_batch_run_async(cosims_batch *b, const uint64_t *seed,
                                      cosims_ccs_sums *d_sums, void *stream);
 cosims_status cosims_batch_get_launch(const cosims_batch *b, int32_t mol,
                                       int32_t *group_lanes, int32_t *item_traj);
+/* Progress interval for the per-molecule n_eff bookkeeping (as update_every
+ * of cosims_run_sampled; default 0). */
+cosims_status cosims_batch_set_update_every(cosims_batch *b, int64_t update_every);
+/* Work of the last run summed over all molecules (steps, evaluations, pair
+ * terms; the CCS fields are 0) and its device time in ms (CUDA events around
+ * the graph launch; ms may be NULL).  Waits for the run.  For measurement. */
+cosims_status cosims_batch_counters(cosims_batch *b, cosims_ccs_sums *work, float *ms);
 
 #ifdef __cplusplus
 }
