@@ -79,6 +79,8 @@ def _bind():
                                          C.c_int64]),
         "cosims_setup_create": (C.c_int, [P(ConfigStruct), C.c_char_p, C.c_char_p, C.c_char_p,
                                           C.c_int64, P(V)]),
+        "cosims_setup_create_device": (C.c_int, [P(ConfigStruct), C.c_char_p, C.c_char_p,
+                                                 C.c_int32, C.c_char_p, C.c_int64, P(V)]),
         "cosims_setup_molecule": (C.c_int, [V, P(abi.Molecule), P(abi.Params)]),
         "cosims_setup_get_info": (C.c_int, [V, P(SetupInfo)]),
         "cosims_setup_boundary": (C.c_int64, [V, V, C.c_int64]),
@@ -128,12 +130,19 @@ class Config:
 class Setup:
     """Per-molecule setup: the molecule and path scalars the kernels consume."""
 
-    def __init__(self, cfg: Config, mol_path: str, atom_path: str | None = None):
+    def __init__(self, cfg: Config, mol_path: str, atom_path: str | None = None,
+                 device: int | None = None):
+        """device: run the boundary ray march on this GPU (same result)."""
         L = _bind()
         h = C.c_void_p()
         buf = C.create_string_buffer(1 << 16)
-        check(L.cosims_setup_create(C.byref(cfg.s), mol_path.encode(),
-                                    (atom_path or "").encode(), buf, len(buf), C.byref(h)))
+        if device is None:
+            check(L.cosims_setup_create(C.byref(cfg.s), mol_path.encode(),
+                                        (atom_path or "").encode(), buf, len(buf), C.byref(h)))
+        else:
+            check(L.cosims_setup_create_device(C.byref(cfg.s), mol_path.encode(),
+                                               (atom_path or "").encode(), int(device), buf,
+                                               len(buf), C.byref(h)))
         self._h = h
         self.log = buf.value.decode(errors="replace")
         m, p = abi.Molecule(), abi.Params()
@@ -174,5 +183,7 @@ class Setup:
 
 
 def setup_from_files(mol_path: str, input_path: str | None = None, atom_path: str | None = None,
-                     seed: int | None = None, threads: int | None = None) -> Setup:
-    return Setup(Config(mol_path, input_path, seed=seed, threads=threads), mol_path, atom_path)
+                     seed: int | None = None, threads: int | None = None,
+                     device: int | None = None) -> Setup:
+    return Setup(Config(mol_path, input_path, seed=seed, threads=threads), mol_path, atom_path,
+                 device=device)

@@ -215,9 +215,9 @@ cosims_status cosims_config_read(cosims_config *c, const char *input_path, const
   return COSIMS_OK;
 }
 
-cosims_status cosims_setup_create(const cosims_config *cfg, const char *mol_path,
-                                  const char *atom_path, char *log_out, int64_t log_cap,
-                                  cosims_setup **out) {
+static cosims_status setup_create(const cosims_config *cfg, const char *mol_path,
+                                  const char *atom_path, int device, char *log_out,
+                                  int64_t log_cap, cosims_setup **out) {
   if (!cfg || !mol_path || !out) return fail(COSIMS_ERR_INVALID, "config, molecule and out are required");
   *out = nullptr;
   Log log;
@@ -277,7 +277,7 @@ cosims_status cosims_setup_create(const cosims_config *cfg, const char *mol_path
   const double minKin = 0.5 * mu * std::pow(vd_mean(2, beta / 2.0) - 2 * vd_std(2, beta / 2.0), 2);
   int threads = cfg->threads > 0 ? cfg->threads : 1;
   if (threads == 1) threads = std::max(1u, std::thread::hardware_concurrency());
-  if (!boundary_scan(m, charged, dipole_scalar, minKin, threads, s->boundary, log)) {
+  if (!boundary_scan(m, charged, dipole_scalar, minKin, threads, device, s->boundary, log)) {
     log.copy_to(log_out, log_cap);
     delete s;
     return fail(COSIMS_ERR_INVALID, "potential-energy boundary scan failed");
@@ -378,6 +378,19 @@ cosims_status cosims_setup_create(const cosims_config *cfg, const char *mol_path
   log.copy_to(log_out, log_cap);
   *out = s;
   return COSIMS_OK;
+}
+
+cosims_status cosims_setup_create(const cosims_config *cfg, const char *mol_path,
+                                  const char *atom_path, char *log_out, int64_t log_cap,
+                                  cosims_setup **out) {
+  return setup_create(cfg, mol_path, atom_path, -1, log_out, log_cap, out);
+}
+
+cosims_status cosims_setup_create_device(const cosims_config *cfg, const char *mol_path,
+                                         const char *atom_path, int32_t device, char *log_out,
+                                         int64_t log_cap, cosims_setup **out) {
+  if (device < 0) return fail(COSIMS_ERR_INVALID, "device must be >= 0");
+  return setup_create(cfg, mol_path, atom_path, device, log_out, log_cap, out);
 }
 
 cosims_status cosims_setup_molecule(const cosims_setup *s, cosims_molecule *m, cosims_params *p) {

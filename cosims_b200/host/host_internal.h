@@ -100,8 +100,25 @@ void fit_ellipsoid(const std::vector<V3> &pts, Ellipsoid &e);
 void enlarge_ellipsoid(const std::vector<V3> &pts, Ellipsoid &e);
 bool form_clusters(const Molecule &m, int maxClusterSize, Clusters &cl, Log &log);
 double potential(const Molecule &m, bool charged, double dipole_scalar, const V3 &pos);
+// impactParam::setBoundry: the z-axis search on the host, the ray march on
+// host threads (device < 0) or on the GPU (boundary_march_gpu).
 bool boundary_scan(const Molecule &m, bool charged, double dipole_scalar, double minKin,
-                   int threads, std::vector<V3> &out, Log &log);
+                   int threads, int device, std::vector<V3> &out, Log &log);
+
+constexpr long kMaxRaySteps = 40000000;   // 4e6 Angstrom of 0.1 A steps; the reference has no cap
+
+// The ray march of impactParam::setBoundry (impactParam.cpp:663-721) on the
+// GPU: one thread per (z level, rotation), the potential summed in file order
+// with IEEE double and no FMA, so the boundary equals the host's bit for bit.
+// Ray starts and directions come from the host (libm cos/sin).  out_xyz:
+// levels * rotations points, (0,0,0) where a ray found none.  Returns 0 on
+// success, else writes a message to err.
+int boundary_march_gpu(int device, int n_atoms, const double *x, const double *y, const double *z,
+                       const double *q, const double *sig6, const double *eps4, int charged,
+                       double dipole_scalar, double min_kin, double z_max, double z_inc,
+                       int levels, int rotations, const double *start_x, const double *start_y,
+                       const double *vel_x, const double *vel_y, double *out_xyz, char *err,
+                       int err_cap);
 
 }  // namespace host
 }  // namespace cosims

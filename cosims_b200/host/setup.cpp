@@ -557,7 +557,7 @@ double vd_cdf(int n, double a, double x) {
 // the slowest kinetic energy.  Rays of one z level are independent; levels are
 // spread over threads.
 bool boundary_scan(const Molecule &m, bool charged, double dipole_scalar, double minKin,
-                   int threads, std::vector<V3> &out, Log &log) {
+                   int threads, int device, std::vector<V3> &out, Log &log) {
   const int numRotations = 20;
   const double velMag = 0.1;
   double posMag = std::fabs(std::max(std::fabs(m.maxX), std::fabs(m.maxY)));
@@ -584,53 +584,80 @@ bool boundary_scan(const Molecule &m, bool charged, double dipole_scalar, double
   posMag += std::fabs(zMax - std::fabs(m.maxZ));
   const int maxZLevels = (int)std::ceil(std::max(25, (int)std::ceil(zMax)));
   const double zInc = 2 * zMax / (maxZLevels);
-  std::vector<V3> tmp((size_t)(maxZLevels + 1) * numRotations, V3(0, 0, 0));
-  std::vector<char> failed(maxZLevels + 1, 0);
-  auto level = [&](int i) {
-    const double zPos = -zMax + i * zInc;
-    V3 prevPos;
-    for (int n = 0; n < numRotations; n++) {
-      double sl = 1;
-      const double theta = n * 2 * kPi / ((double)numRotations);
-      const double startX = posMag * std::cos(theta);
-      const double startY = posMag * std::sin(theta);
-      V3 p(startX, startY, zPos);
-      V3 vel(-velMag * std::cos(theta), -velMag * std::sin(theta), 0.0);
-      double e = potential(m, charged, dipole_scalar, p);
-      if (e + minKin < 0) sl = -1;
-      vel = vel * sl;
-      for (long step = 0;; step++) {
-        e = potential(m, charged, dipole_scalar, p);
-        if ((e + minKin) * sl < 0) {
-          tmp[(size_t)i * numRotations + n] = prevPos.mag() > p.mag() ? prevPos : p;
-          break;
-        } else if ((startX == 0 && startY / p.Y <= 0) || (startY == 0 && startX / p.X <= 0) ||
-                   (startX / p.X <= 0 && startY / p.Y <= 0)) {
-          break;
-        }
-        prevPos = p;
-        p = p + vel;
-        if (step > 40000000) { failed[i] = 1; return; }
-      }
-    }
-  };
-  int nt = std::max(1, threads);
-  nt = std::min(nt, maxZLevels + 1);
-  if (nt == 1) {
-    for (int i = 0; i <= maxZLevels; i++) level(i);
-  } else {
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nt; t++)
-      pool.emplace_back([&, t]() {
-        for (int i = t; i <= maxZLevels; i += nt) level(i);
-      });
-    for (auto &th : pool) th.join();
+  // ray directions with the host's libm, as the reference computes them
+  std::vector<double> sx(numRotations), sy(numRotations), vx(numRotations), vy(numRotations);
+  for (int n = 0; n < numRotations; n++) {
+    const double theta = n * 2 * kPi / ((double)numRotations);
+    sx[n] = posMag * std::cos(theta);
+    sy[n] = posMag * std::sin(theta);
+    vx[n] = -velMag * std::cos(theta);
+    vy[n] = -velMag * std::sin(theta);
   }
-  for (char f : failed)
-    if (f) {
-      log.printf("Error: a boundary ray did not terminate\n");
+  std::vector<V3> tmp((size_t)(maxZLevels + 1) * numRotations, V3(0, 0, 0));
+  if (device >= 0) {
+    // the ray march on the GPU (one thread per ray, the same IEEE sequence)
+    const int n = (int)m.atoms.size();
+    std::vector<double> x(n), y(n), z(n), q(n), s6(n), e4(n);
+    for (int k = 0; k < n; k++) {
+      x[k] = m.atoms[k].x; y[k] = m.atoms[k].y; z[k] = m.atoms[k].z;
+      q[k] = m.atoms[k].charge; s6[k] = m.atoms[k].sig6; e4[k] = m.atoms[k].eps4;
+    }
+    std::vector<double> xyz(tmp.size() * 3, 0.0);
+    char err[256] = {0};
+    if (boundary_march_gpu(device, n, x.data(), y.data(), z.data(), q.data(), s6.data(),
+                           e4.data(), charged ? 1 : 0, dipole_scalar, minKin, zMax, zInc,
+                           maxZLevels + 1, numRotations, sx.data(), sy.data(), vx.data(),
+                           vy.data(), xyz.data(), err, sizeof err) != 0) {
+      log.printf("Error: device boundary scan: %s\n", err);
       return false;
     }
+    for (size_t k = 0; k < tmp.size(); k++) tmp[k] = V3(xyz[3 * k], xyz[3 * k + 1], xyz[3 * k + 2]);
+  } else {
+    std::vector<char> failed(maxZLevels + 1, 0);
+    auto level = [&](int i) {
+      const double zPos = -zMax + i * zInc;
+      V3 prevPos;
+      for (int n = 0; n < numRotations; n++) {
+        double sl = 1;
+        const double startX = sx[n], startY = sy[n];
+        V3 p(startX, startY, zPos);
+        V3 vel(vx[n], vy[n], 0.0);
+        double e = potential(m, charged, dipole_scalar, p);
+        if (e + minKin < 0) sl = -1;
+        vel = vel * sl;
+        for (long step = 0;; step++) {
+          e = potential(m, charged, dipole_scalar, p);
+          if ((e + minKin) * sl < 0) {
+            tmp[(size_t)i * numRotations + n] = prevPos.mag() > p.mag() ? prevPos : p;
+            break;
+          } else if ((startX == 0 && startY / p.Y <= 0) || (startY == 0 && startX / p.X <= 0) ||
+                     (startX / p.X <= 0 && startY / p.Y <= 0)) {
+            break;
+          }
+          prevPos = p;
+          p = p + vel;
+          if (step > kMaxRaySteps) { failed[i] = 1; return; }
+        }
+      }
+    };
+    int nt = std::max(1, threads);
+    nt = std::min(nt, maxZLevels + 1);
+    if (nt == 1) {
+      for (int i = 0; i <= maxZLevels; i++) level(i);
+    } else {
+      std::vector<std::thread> pool;
+      for (int t = 0; t < nt; t++)
+        pool.emplace_back([&, t]() {
+          for (int i = t; i <= maxZLevels; i += nt) level(i);
+        });
+      for (auto &th : pool) th.join();
+    }
+    for (char f : failed)
+      if (f) {
+        log.printf("Error: a boundary ray did not terminate\n");
+        return false;
+      }
+  }
   out.clear();
   for (const V3 &p : tmp)
     if (!(p.X == 0 && p.Y == 0 && p.Z == 0)) out.push_back(p);

@@ -98,6 +98,13 @@ typedef struct cosims_setup_info {
 cosims_status cosims_setup_create(const cosims_config *cfg, const char *mol_path,
                                   const char *atom_path, char *log, int64_t log_cap,
                                   cosims_setup **out);
+/* The same setup with the boundary ray march (impactParam::setBoundry's
+ * OpenMP loop, impactParam.cpp:661-721) on `device`: one GPU thread per ray,
+ * the same IEEE operation sequence, so the result equals cosims_setup_create's
+ * bit for bit.  For serving and batches, where host setup time dominates. */
+cosims_status cosims_setup_create_device(const cosims_config *cfg, const char *mol_path,
+                                         const char *atom_path, int32_t device, char *log,
+                                         int64_t log_cap, cosims_setup **out);
 /* Views of the setup's molecule and path scalars (valid while the setup
  * lives); feed them to cosims_ctx_create. */
 cosims_status cosims_setup_molecule(const cosims_setup *s, cosims_molecule *mol,

@@ -67,3 +67,17 @@ def test_batch_autotune_and_graph_replay():
         assert [x.sum for x in r1] == [x.sum for x in r2]
         r3 = b.run(seeds, first, n + 17)     # new shape: captured again
         assert all(x.n == 2017 for x in r3)
+
+
+def test_device_boundary_scan_equals_host(tmp_path):
+    """cosims_setup_create_device: the ray march on the GPU gives the host's
+    boundary, ellipsoid and path scalars bit for bit."""
+    from cosims_b200 import host, synth
+    from tests.golden.make_golden import charged128
+    for mol, force in ((synth.config1_molecule(), "cutoff"), (charged128(), "multipole12"),
+                       (synth.config0_molecule(), "cutoff")):
+        mp, ip = synth.write_case(str(tmp_path), mol, force)
+        a = host.setup_from_files(mp, ip, seed=1)
+        b = host.setup_from_files(mp, ip, seed=1, device=0)
+        np.testing.assert_array_equal(a.boundary, b.boundary)
+        assert abi.params_to_dict(a.params) == abi.params_to_dict(b.params)
