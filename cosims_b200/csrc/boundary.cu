@@ -82,6 +82,7 @@ __global__ void boundary_rays(const RayAtoms m, int charged, double ds, double m
   out[3 * r + 2] = oz;
 }
 
+namespace host {
 int boundary_march_gpu(int device, int n_atoms, const double *x, const double *y, const double *z,
                        const double *q, const double *sig6, const double *eps4, int charged,
                        double dipole_scalar, double min_kin, double z_max, double z_inc,
@@ -138,5 +139,6 @@ int boundary_march_gpu(int device, int n_atoms, const double *x, const double *y
   }
   return 0;
 }
+}  // namespace host
 
 }  // namespace cosims
