@@ -183,3 +183,12 @@ def params_from_dict(d: dict) -> Params:
         v = d[k]
         setattr(p, k, int(v) if t in (C.c_int32, C.c_int64) else float(v))
     return p
+
+
+JOB_RUNNING, JOB_DONE = 1, 2
+
+
+class JobStatus(C.Structure):
+    _fields_ = [("job_id", C.c_int64), ("state", C.c_int32), ("rounds", C.c_int32),
+                ("omega", C.c_double), ("se", C.c_double), ("rel_se", C.c_double),
+                ("device_ms", C.c_double), ("sums", CcsSums)]

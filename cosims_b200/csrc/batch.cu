@@ -42,6 +42,15 @@ int mode_stride_of(const MolImage &img) {
 }
 
 }  // namespace
+
+// Lanes per trajectory for a molecule: the tuned value of its size class if
+// cosims_batch_autotune has measured one in this process, else the default.
+int tuned_group_lanes(int type, int n_atoms) {
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  auto it = g_tune.find({type, size_class(n_atoms)});
+  return it != g_tune.end() ? it->second : default_group_lanes(n_atoms);
+}
+
 }  // namespace cosims
 
 using namespace cosims;

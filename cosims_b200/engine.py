@@ -66,6 +66,14 @@ def lib():
                 "cosims_batch_set_update_every": (st, [V, C.c_int64]),
                 "cosims_batch_counters": (st, [V, P(abi.CcsSums), P(C.c_float)]),
                 "cosims_ctx_kernel_ms": (st, [V, P(C.c_float)]),
+                "cosims_serve_create": (st, [C.c_int32, C.c_int64, C.c_int32, C.c_int64, P(V)]),
+                "cosims_serve_destroy": (None, [V]),
+                "cosims_serve_submit": (st, [V, P(abi.Molecule), P(abi.Params), C.c_uint64,
+                                             C.c_double, C.c_int64, C.c_int64, P(C.c_int64)]),
+                "cosims_serve_step": (st, [V, V, P(C.c_int32)]),
+                "cosims_serve_poll": (st, [V, C.c_int64, P(abi.JobStatus)]),
+                "cosims_serve_release": (st, [V, C.c_int64]),
+                "cosims_serve_info": (st, [V, P(C.c_int32), P(C.c_int64)]),
                 "cosims_probe_peaks": (st, [C.c_int32, P(C.c_double), P(C.c_double)]),
             }
             for name, (res, args) in sig.items():
@@ -249,6 +257,68 @@ class Batch:
         w, ms = abi.CcsSums(), C.c_float()
         check(lib().cosims_batch_counters(self._h, C.byref(w), C.byref(ms)))
         return w, ms.value
+
+
+class Server:
+    """Continuous-batching CCS service: jobs admitted by HBM footprint, each
+    molecule and its running sums resident on the device until released."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 8 << 30, max_jobs: int = 64,
+                 round_traj: int = 16384):
+        h = C.c_void_p()
+        check(lib().cosims_serve_create(device, int(hbm_budget), int(max_jobs), int(round_traj),
+                                        C.byref(h)))
+        self._h = h
+        self.round_traj = round_traj
+        self._keep = {}
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            lib().cosims_serve_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def submit(self, mol: abi.MoleculeArrays, par: abi.Params, seed: int, target_rel_se: float,
+               min_traj: int = 0, max_traj: int = 1 << 40):
+        """Job id, or None when the server has no room now (admission)."""
+        view = mol.view()
+        jid = C.c_int64()
+        st = lib().cosims_serve_submit(self._h, C.byref(view), C.byref(par), int(seed),
+                                       float(target_rel_se), int(min_traj), int(max_traj),
+                                       C.byref(jid))
+        if st == abi.ERR_BUSY:
+            return None
+        check(st)
+        return jid.value
+
+    def step(self, stream=None) -> int:
+        n = C.c_int32()
+        check(lib().cosims_serve_step(self._h, _stream_ptr(stream), C.byref(n)))
+        return n.value
+
+    def poll(self, job_id: int) -> abi.JobStatus:
+        s = abi.JobStatus()
+        check(lib().cosims_serve_poll(self._h, job_id, C.byref(s)))
+        return s
+
+    def release(self, job_id: int) -> None:
+        check(lib().cosims_serve_release(self._h, job_id))
+
+    def info(self) -> tuple:
+        a, b = C.c_int32(), C.c_int64()
+        check(lib().cosims_serve_info(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
 
 
 def probe_peaks(device: int = 0) -> tuple:

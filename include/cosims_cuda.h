@@ -288,6 +288,44 @@ cosims_status cosims_batch_set_update_every(cosims_batch *b, int64_t update_ever
  * the graph launch; ms may be NULL).  Waits for the run.  For measurement. */
 cosims_status cosims_batch_counters(cosims_batch *b, cosims_ccs_sums *work, float *ms);
 
+/* ---- serving: continuous batching of CCS jobs ---------------------------- */
+/* No counterpart in the reference (it computes one molecule per process).
+ * Jobs are admitted while their device footprint fits the HBM budget and a
+ * slot is free; each job's molecule and running sums stay on the device.  A
+ * round integrates the next round_traj trajectories of every running job in
+ * one persistent launch and retires jobs whose relative standard error
+ * reached their target (or that reached max_traj).  A job's k-th round is
+ * always trajectories [k*round_traj, (k+1)*round_traj) of its own stream, so
+ * its result does not depend on the other jobs. */
+typedef struct cosims_server cosims_server;
+
+#define COSIMS_JOB_RUNNING 1
+#define COSIMS_JOB_DONE 2
+
+typedef struct cosims_job_status {
+    int64_t job_id;
+    int32_t state;            /* COSIMS_JOB_*                                     */
+    int32_t rounds;           /* rounds integrated                                */
+    double omega, se, rel_se; /* running CCS (Omega = sum / n_eff) and its error  */
+    double device_ms;         /* submit -> retirement, host clock (done jobs)     */
+    cosims_ccs_sums sums;     /* running sums                                     */
+} cosims_job_status;
+
+cosims_status cosims_serve_create(int32_t device, int64_t hbm_budget_bytes, int32_t max_jobs,
+                                  int64_t round_traj, cosims_server **out);
+void cosims_serve_destroy(cosims_server *s);
+/* Admits a job, or returns COSIMS_ERR_BUSY when it does not fit now. */
+cosims_status cosims_serve_submit(cosims_server *s, const cosims_molecule *mol,
+                                  const cosims_params *par, uint64_t seed, double target_rel_se,
+                                  int64_t min_traj, int64_t max_traj, int64_t *job_id);
+/* One round over all running jobs on `stream`; waits for it.  n_finished:
+ * jobs that retired in this round. */
+cosims_status cosims_serve_step(cosims_server *s, void *stream, int32_t *n_finished);
+cosims_status cosims_serve_poll(cosims_server *s, int64_t job_id, cosims_job_status *out);
+/* Frees a job's device resources (its slot and footprint return to the pool). */
+cosims_status cosims_serve_release(cosims_server *s, int64_t job_id);
+cosims_status cosims_serve_info(const cosims_server *s, int32_t *active, int64_t *bytes_in_use);
+
 #ifdef __cplusplus
 }
 #endif
