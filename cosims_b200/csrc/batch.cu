@@ -21,7 +21,7 @@ namespace cosims {
 namespace {
 
 constexpr uint32_t kBatchImageCap = 96 * 1024;   // larger F32 images are read through L1/L2
-constexpr int kBatchBlock = 256;
+constexpr int kBatchBlock = kBatchMaxBlock;
 constexpr int kTrajPerGroupPerItem = 16;
 
 // process-wide tuning cache: (force type, atom-count class) -> lanes per trajectory
@@ -34,14 +34,24 @@ int size_class(int n_atoms) {
   return c;
 }
 
-int mode_stride_of(const MolImage &img) {
-  if (!img.uses_clusters) return 0;
-  int s = (img.n_clusters + 3) & ~3;
-  if (((s / 4) & 1) == 0) s += 4;
-  return s;
-}
-
 }  // namespace
+
+// Dynamic shared memory one batched-kernel CTA of `block` threads needs for
+// molecule bm: its F32 image when staged (at most img_cap bytes, and only if
+// it fits the budget) plus each group's trajectory state and mode scratch.
+// Sets bm.use_smem and bm.mode_stride.
+size_t batch_mol_smem(BatchMol &bm, int block, int budget, uint32_t img_cap) {
+  bm.use_smem = bm.img32.bytes <= img_cap ? 1 : 0;
+  bm.mode_stride = mode_stride_for(bm.img32);
+  const size_t groups = (size_t)(block / bm.group_lanes);
+  const size_t scratch = groups * ((size_t)kGroupStateBytes + (size_t)bm.mode_stride);
+  size_t need = (bm.use_smem ? ((bm.img32.bytes + 15u) & ~15u) : 0) + scratch;
+  if ((int)need > budget && bm.use_smem) {
+    bm.use_smem = 0;
+    need = scratch;
+  }
+  return need;
+}
 
 // Lanes per trajectory for a molecule: the tuned value of its size class if
 // cosims_batch_autotune has measured one in this process, else the default.
@@ -90,14 +100,7 @@ cosims_status shape_launch(cosims_batch *b) {
   size_t smem = 0;
   for (int m = 0; m < b->n_mol; m++) {
     BatchMol &bm = b->mols[m];
-    bm.use_smem = bm.img32.bytes <= kBatchImageCap ? 1 : 0;
-    bm.mode_stride = mode_stride_of(bm.img32);
-    size_t need = (bm.use_smem ? bm.img32.bytes : 0) +
-                  (size_t)(kBatchBlock / bm.group_lanes) * bm.mode_stride;
-    if ((int)need > budget && bm.use_smem) {
-      bm.use_smem = 0;
-      need = (size_t)(kBatchBlock / bm.group_lanes) * bm.mode_stride;
-    }
+    const size_t need = batch_mol_smem(bm, kBatchBlock, budget, kBatchImageCap);
     if ((int)need > budget)
       return fail(COSIMS_ERR_UNSUPPORTED, "molecule %d needs %zu bytes of shared memory", m, need);
     smem = std::max(smem, need);

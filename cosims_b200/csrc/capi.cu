@@ -5,6 +5,7 @@
 #include <climits>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -126,10 +127,12 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   }
   for (int k = 0; k < n; k++) perm[order[k]] = k;
 
+  // F32 arrays padded to a multiple of kSlotQuantum with inert atoms
+  const int ns = (n + kSlotQuantum - 1) / kSlotQuantum * kSlotQuantum;
   std::vector<AtomF64> a64(n);
-  std::vector<float4> a4(n);
-  std::vector<float2> lj2(n);
-  std::vector<uint16_t> cid16(n);
+  std::vector<float4> a4(ns, make_float4(kPadCoord, kPadCoord, kPadCoord, 0.0f));
+  std::vector<float2> lj2(ns, make_float2(0.0f, 0.0f));
+  std::vector<uint16_t> cid16(ns, (uint16_t)nc);
   for (int k = 0; k < n; k++) {
     const int i = order[k];
     AtomF64 &A = a64[k];
@@ -178,6 +181,7 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   b64.finish();
   i64.bytes = (uint32_t)b64.buf.size();
   i64.n_atoms = n;
+  i64.n_slots = n;
   i64.n_clusters = nc;
   i64.uses_clusters = uses ? 1 : 0;
   h64.bytes = std::move(b64.buf);
@@ -185,13 +189,14 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   Builder b32;
   MolImage &i32 = h32.img;
   std::memset(&i32, 0, sizeof i32);
-  i32.off[S_ATOMS] = b32.add(a4.data(), sizeof(float4) * n);
-  i32.off[S_LJ] = b32.add(lj2.data(), sizeof(float2) * n);
-  i32.off[S_CID] = b32.add(cid16.data(), sizeof(uint16_t) * n);
+  i32.off[S_ATOMS] = b32.add(a4.data(), sizeof(float4) * ns);
+  i32.off[S_LJ] = b32.add(lj2.data(), sizeof(float2) * ns);
+  i32.off[S_CID] = b32.add(cid16.data(), sizeof(uint16_t) * ns);
   i32.off[S_CLUSTERS] = b32.add(c32.data(), sizeof(ClusterF32) * nc);
   b32.finish();
   i32.bytes = (uint32_t)b32.buf.size();
   i32.n_atoms = n;
+  i32.n_slots = ns;
   i32.n_clusters = nc;
   i32.uses_clusters = uses ? 1 : 0;
   h32.bytes = std::move(b32.buf);
@@ -237,41 +242,123 @@ static cosims_status grow(T **p, int64_t *cap, int64_t need) {
   return COSIMS_OK;
 }
 
-// Launch shape for a context: threads per CTA, CTAs, dynamic shared memory,
-// whether the image is staged, and the per-group mode scratch.
-cosims_status launch_shape(const cosims_ctx *c, int64_t n, LaunchShape &ls) {
-  const int G = c->precision == COSIMS_PRECISION_PLAIN_F64 ? 1 : c->group_lanes;
-  int block = c->block_threads;
-  const MolImage &img = c->precision == COSIMS_PRECISION_PLAIN_F64 ? c->img64 : c->img32;
-  const int budget = c->max_smem - 1024;
-  ls.use_smem = (int)img.bytes <= budget ? 1 : 0;
-  ls.mode_stride = 0;
-  if (c->precision == COSIMS_PRECISION_MIXED && img.uses_clusters) {
-    int s = (img.n_clusters + 3) & ~3;
-    if (((s / 4) & 1) == 0) s += 4;     // odd word count: groups hit distinct banks
-    ls.mode_stride = s;
+// Shared-memory bytes of one mixed-form group: its trajectory state and its
+// cluster-mode scratch (n_clusters + 1 bytes: the last entry, always 0,
+// belongs to the pad atoms).
+int mode_stride_for(const MolImage &img) {
+  if (!img.uses_clusters) return 0;
+  int s = (img.n_clusters + 1 + 3) & ~3;
+  if (((s / 4) & 1) == 0) s += 4;     // odd word count: groups hit distinct banks
+  return s;
+}
+
+// Launch shape: threads per CTA, CTAs, dynamic shared memory, whether the
+// image is staged, and the per-group mode scratch.  block_threads 0 (mixed
+// form) picks the CTA size (256, 512, 768 or 1024 threads) that keeps the
+// most threads resident per SM, preferring a staged image: one staged copy of
+// the molecule serves every group of a CTA.
+cosims_status shape_for(bool plain, const MolImage &img, int G, int block_threads,
+                        int wide_lanes, int force_type, int sm_count, int max_smem, int64_t n,
+                        LaunchShape &ls) {
+  const int budget = max_smem - 1024;
+  const int stride = plain ? 0 : mode_stride_for(img);
+  const size_t per_group = plain ? 0 : (size_t)kGroupStateBytes + (size_t)stride;
+  const size_t per_wide = (!plain && wide_lanes > 0) ? wide_group_bytes(wide_lanes, stride) : 0;
+  const size_t img_bytes = (img.bytes + 15u) & ~15u;
+  int cands[4] = {block_threads, 0, 0, 0};
+  int ncand = 1;
+  if (!plain && block_threads == 0) {
+    cands[0] = 256; cands[1] = 512; cands[2] = kMixedMaxBlock;
+    ncand = 3;
   }
-  // shrink the CTA until image + mode scratch fit
-  for (;;) {
-    size_t smem = (ls.use_smem ? img.bytes : 0) + (size_t)(block / G) * ls.mode_stride;
-    if ((int)smem <= budget) { ls.smem = smem; break; }
-    if (ls.use_smem && block <= std::max(G, 32)) { ls.use_smem = 0; continue; }
-    if (block <= std::max(G, 32))
-      return fail(COSIMS_ERR_UNSUPPORTED, "molecule image does not fit in shared memory");
-    block /= 2;
+  bool found = false;
+  int best_resident = -1;
+  for (int ci = 0; ci < ncand; ci++) {
+    int block = cands[ci];
+    if (block < G) continue;
+    LaunchShape t;
+    t.use_smem = (int)img_bytes <= budget ? 1 : 0;
+    t.mode_stride = stride;
+    // shrink the CTA until image + group scratch fit
+    bool ok = true;
+    for (;;) {
+      size_t scratch = (size_t)(block / G) * per_group;
+      // wide phase: whole wide groups only, at most 15 (named barriers 1..15)
+      t.wide_lanes = (per_wide && block >= wide_lanes && block / wide_lanes <= 15) ? wide_lanes : 0;
+      if (t.wide_lanes) scratch = std::max(scratch, (size_t)(block / wide_lanes) * per_wide);
+      size_t smem = (t.use_smem ? img_bytes : 0) + scratch;
+      if ((int)smem <= budget) { t.smem = smem; break; }
+      if (t.use_smem && block <= std::max(G, 32)) { t.use_smem = 0; continue; }
+      if (block <= std::max(G, 32)) { ok = false; break; }
+      block /= 2;
+    }
+    if (!ok) continue;
+    t.block = block;
+    int per_sm = 0;
+    int rc = plain ? plain_occupancy(block, t.smem, &per_sm)
+                   : mixed_occupancy(force_type, t.use_smem, block, t.smem, &per_sm);
+    if (rc != 0) return cuda_fail((cudaError_t)rc, "occupancy query");
+    if (per_sm <= 0) continue;          // over the kernel's thread or register limit
+    const int resident = per_sm * block * (t.use_smem ? 2 : 1);
+    if (resident > best_resident) {
+      best_resident = resident;
+      t.grid = per_sm;                  // CTAs per SM until the grid is sized below
+      ls = t;
+      found = true;
+    }
   }
-  ls.block = block;
-  int per_sm = 1;
-  int rc = c->precision == COSIMS_PRECISION_PLAIN_F64
-               ? plain_occupancy(block, ls.smem, &per_sm)
-               : mixed_occupancy(c->par.force_type, block, ls.smem, &per_sm);
-  if (rc != 0) return cuda_fail((cudaError_t)rc, "occupancy query");
-  per_sm = std::max(per_sm, 1);
-  const int64_t groups_needed = n;   // one group per trajectory at most
-  const int64_t groups_per_cta = block / G;
-  int64_t grid = (int64_t)per_sm * c->sm_count;
-  grid = std::min<int64_t>(grid, (groups_needed + groups_per_cta - 1) / groups_per_cta);
+  if (!found) return fail(COSIMS_ERR_UNSUPPORTED, "molecule image does not fit in shared memory");
+  const int64_t groups_per_cta = ls.block / G;
+  int64_t grid = (int64_t)ls.grid * sm_count;
+  grid = std::min<int64_t>(grid, (n + groups_per_cta - 1) / groups_per_cta);
   ls.grid = (int)std::max<int64_t>(grid, 1);
+  return COSIMS_OK;
+}
+
+int ctx_wide_lanes(const cosims_ctx *c) {
+  if (c->precision != COSIMS_PRECISION_MIXED || c->ho_budget <= 0) return 0;
+  return c->ho_wide > 0 ? c->ho_wide : default_wide_lanes(c->n_atoms);
+}
+
+cosims_status launch_shape(const cosims_ctx *c, int64_t n, LaunchShape &ls) {
+  const bool plain = c->precision == COSIMS_PRECISION_PLAIN_F64;
+  return shape_for(plain, plain ? c->img64 : c->img32, plain ? 1 : c->group_lanes,
+                   c->block_threads, ctx_wide_lanes(c), c->par.force_type, c->sm_count,
+                   c->max_smem, n, ls);
+}
+
+// Hand-off buffers for n trajectories: one record per 16 trajectories (at
+// least 256), ready flags and counters cleared on the stream.
+cosims_status handoff_prepare(cosims_ctx *c, int64_t n, const LaunchShape &ls, Handoff &ho,
+                              cudaStream_t s) {
+  std::memset(&ho, 0, sizeof ho);
+  if (!ls.wide_lanes || n == 0) return COSIMS_OK;
+  const int64_t want = std::min<int64_t>(std::max<int64_t>(256, n / 16), 1 << 20);
+  if (c->ho_cap < want) {
+    cudaFree(c->d_ho_states);
+    cudaFree(c->d_ho_ready);
+    c->d_ho_states = nullptr;
+    c->d_ho_ready = nullptr;
+    c->ho_cap = 0;
+    cudaError_t e = cudaMalloc((void **)&c->d_ho_states, sizeof(TrajState) * (size_t)want);
+    if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_ho_ready, sizeof(uint32_t) * (size_t)want);
+    if (e != cudaSuccess) return fail(COSIMS_ERR_NOMEM, "hand-off buffers: %s", cudaGetErrorString(e));
+    c->ho_cap = want;
+  }
+  if (!c->d_ho_ctrl) {
+    cudaError_t e = cudaMalloc((void **)&c->d_ho_ctrl, 2 * sizeof(unsigned long long));
+    if (e != cudaSuccess) return fail(COSIMS_ERR_NOMEM, "hand-off counters: %s", cudaGetErrorString(e));
+  }
+  cudaError_t e = cudaMemsetAsync(c->d_ho_ready, 0, sizeof(uint32_t) * (size_t)c->ho_cap, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_ho_ctrl, 0, 2 * sizeof(unsigned long long), s);
+  if (e != cudaSuccess) return cuda_fail(e, "hand-off reset");
+  ho.states = c->d_ho_states;
+  ho.ready = c->d_ho_ready;
+  ho.reserve = c->d_ho_ctrl;
+  ho.taken = c->d_ho_ctrl + 1;
+  ho.cap = c->ho_cap;
+  ho.budget = c->ho_budget;
+  ho.wide_lanes = ls.wide_lanes;
   return COSIMS_OK;
 }
 
@@ -311,6 +398,10 @@ cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0
   a.out = d_out;
   a.queue = c->d_queue;
   a.counters = c->d_counters;
+  if (!plain) {
+    st = handoff_prepare(c, n, ls, a.ho, s);
+    if (st != COSIMS_OK) return st;
+  }
   if (!c->ev0) {
     e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
@@ -391,7 +482,7 @@ cosims_status cosims_ctx_create(const cosims_molecule *mol, const cosims_params 
   c->img64 = c->h64.img;
   c->img32 = c->h32.img;
   c->group_lanes = precision == COSIMS_PRECISION_PLAIN_F64 ? 1 : default_group_lanes(mol->n_atoms);
-  c->block_threads = precision == COSIMS_PRECISION_PLAIN_F64 ? 128 : 256;
+  c->block_threads = precision == COSIMS_PRECISION_PLAIN_F64 ? 128 : 0;   // 0: chosen per run
   cudaError_t e = cudaMalloc((void **)&c->d_img64, c->img64.bytes);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_img32, c->img32.bytes);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_queue, sizeof(unsigned long long));
@@ -430,6 +521,9 @@ void cosims_ctx_destroy(cosims_ctx *c) {
   cudaFree(c->d_hit);
   cudaFree(c->d_order);
   cudaFree(c->d_order_scratch);
+  cudaFree(c->d_ho_states);
+  cudaFree(c->d_ho_ready);
+  cudaFree(c->d_ho_ctrl);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   delete c;
@@ -445,6 +539,52 @@ cosims_status cosims_ctx_kernel_ms(cosims_ctx *c, float *ms) {
   return COSIMS_OK;
 }
 
+cosims_status cosims_ctx_kernel_timeline(cosims_ctx *c, double *drain_ms, double *end_ms) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (!c->timed) return fail(COSIMS_ERR_INVALID, "no trajectory kernel has run on this context");
+  DeviceGuard g(c->device);
+  unsigned long long t[3];
+  cudaError_t e = cudaEventSynchronize(c->ev1);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(t, c->d_counters + C_T_START_INV, sizeof t, cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_fail(e, "kernel timeline");
+  const unsigned long long t0 = ~t[0], td = ~t[1], te = t[2];
+  if (drain_ms) *drain_ms = t[1] ? (double)(long long)(td - t0) * 1e-6 : 0.0;
+  if (end_ms) *end_ms = (double)(long long)(te - t0) * 1e-6;
+  return COSIMS_OK;
+}
+
+cosims_status cosims_ctx_set_handoff(cosims_ctx *c, int64_t step_budget, int32_t wide_lanes) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (c->precision != COSIMS_PRECISION_MIXED)
+    return fail(COSIMS_ERR_INVALID, "the hand-off belongs to the mixed form");
+  if (wide_lanes < 0 || wide_lanes > 512 || (wide_lanes & 31))
+    return fail(COSIMS_ERR_INVALID, "wide_lanes must be 0 or a multiple of 32 up to 512");
+  c->ho_budget = step_budget == 0 ? kDefaultHandoffBudget : (step_budget < 0 ? 0 : step_budget);
+  c->ho_wide = wide_lanes;
+  return COSIMS_OK;
+}
+
+cosims_status cosims_ctx_get_handoff(cosims_ctx *c, int64_t *step_budget, int32_t *wide_lanes,
+                                     int64_t *parked, int64_t *wide_steps, double *wide_ms) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (step_budget) *step_budget = c->ho_budget;
+  if (wide_lanes) *wide_lanes = c->last_shape.wide_lanes ? c->last_shape.wide_lanes : ctx_wide_lanes(c);
+  unsigned long long r = 0, w[2] = {0, 0};
+  if (c->d_ho_ctrl && c->timed && c->last_shape.wide_lanes) {
+    DeviceGuard g(c->device);
+    cudaError_t e = cudaEventSynchronize(c->ev1);
+    if (e == cudaSuccess) e = cudaMemcpy(&r, c->d_ho_ctrl, sizeof r, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(w, c->d_counters + C_WIDE_STEPS, sizeof w, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "hand-off statistics");
+  }
+  if (parked) *parked = (int64_t)std::min<unsigned long long>(r, (unsigned long long)c->ho_cap);
+  if (wide_steps) *wide_steps = (int64_t)w[0];
+  if (wide_ms) *wide_ms = (double)w[1] * 1e-6;
+  return COSIMS_OK;
+}
+
 cosims_status cosims_ctx_set_launch(cosims_ctx *c, int32_t group_lanes, int32_t block_threads) {
   if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
   if (group_lanes) {
@@ -455,12 +595,12 @@ cosims_status cosims_ctx_set_launch(cosims_ctx *c, int32_t group_lanes, int32_t 
     c->group_lanes = group_lanes;
   }
   if (block_threads) {
-    const int maxb = c->precision == COSIMS_PRECISION_PLAIN_F64 ? 128 : 256;
+    const int maxb = c->precision == COSIMS_PRECISION_PLAIN_F64 ? 128 : kMixedMaxBlock;
     if (block_threads < 32 || block_threads > maxb || (block_threads & 31))
       return fail(COSIMS_ERR_INVALID, "block_threads must be a multiple of 32 in 32..%d", maxb);
     c->block_threads = block_threads;
   }
-  if (c->block_threads < c->group_lanes)
+  if (c->block_threads && c->block_threads < c->group_lanes)
     return fail(COSIMS_ERR_INVALID, "block_threads smaller than group_lanes");
   return COSIMS_OK;
 }
@@ -469,7 +609,8 @@ cosims_status cosims_ctx_get_launch(const cosims_ctx *c, int32_t *group_lanes,
                                     int32_t *block_threads) {
   if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
   if (group_lanes) *group_lanes = c->precision == COSIMS_PRECISION_PLAIN_F64 ? 1 : c->group_lanes;
-  if (block_threads) *block_threads = c->block_threads;
+  if (block_threads)
+    *block_threads = c->block_threads ? c->block_threads : c->last_shape.block;
   return COSIMS_OK;
 }
 

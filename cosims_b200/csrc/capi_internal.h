@@ -15,6 +15,7 @@ struct HostImage {
 
 struct LaunchShape {
   int block = 0, grid = 0, use_smem = 0, mode_stride = 0;
+  int wide_lanes = 0;   // mixed form: threads of a hand-off wide group (0: no wide phase)
   size_t smem = 0;
 };
 
@@ -24,6 +25,11 @@ cosims_status validate(const cosims_molecule *mol, const cosims_params *par);
 DevParams make_dev_params(const cosims_params *p);
 void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h64,
                   HostImage &h32);
+int mode_stride_for(const MolImage &img);
+size_t batch_mol_smem(BatchMol &bm, int block, int budget, uint32_t img_cap);
+cosims_status shape_for(bool plain, const MolImage &img, int G, int block_threads,
+                        int wide_lanes, int force_type, int sm_count, int max_smem, int64_t n,
+                        LaunchShape &ls);
 cosims_status check_device(int device, int *sm_count, int *max_smem);
 
 struct DeviceGuard {
@@ -33,7 +39,7 @@ struct DeviceGuard {
 };
 
 int plain_occupancy(int block, size_t smem, int *per_sm);
-int mixed_occupancy(int force_type, int block, size_t smem, int *per_sm);
+int mixed_occupancy(int force_type, int use_smem, int block, size_t smem, int *per_sm);
 
 // Lanes per trajectory before any tuning: enough lanes that a 32-lane warp
 // still holds several trajectories for small molecules, a full warp for large.
@@ -74,6 +80,14 @@ struct cosims_ctx {
   int64_t order_cap = 0;
   int32_t *d_order_scratch = nullptr;
   int64_t order_scratch_cap = 0;
+  // long-trajectory hand-off (mixed form)
+  int64_t ho_budget = cosims::kDefaultHandoffBudget;   // <= 0: off
+  int ho_wide = 0;                                     // 0: default for the molecule
+  cosims::TrajState *d_ho_states = nullptr;
+  uint32_t *d_ho_ready = nullptr;
+  int64_t ho_cap = 0;
+  unsigned long long *d_ho_ctrl = nullptr;             // reserve, taken
+  int64_t ho_last_parked = 0;
   cosims::LaunchShape last_shape{};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // around the last trajectory kernel
   bool timed = false;

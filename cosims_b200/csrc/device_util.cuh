@@ -197,4 +197,19 @@ __device__ __forceinline__ void count_add(unsigned long long *c, int k, long lon
   if (v) atomicAdd(c + k, (unsigned long long)v);
 }
 
+// ---- kernel timeline (globaltimer, ns) -----------------------------------------
+// Counters start at 0, so the earliest-time marks keep the complement under
+// atomicMax.
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ void mark_first(unsigned long long *c, int k) {
+  atomicMax(c + k, ~global_ns());
+}
+__device__ __forceinline__ void mark_last(unsigned long long *c, int k) {
+  atomicMax(c + k, global_ns());
+}
+
 }  // namespace cosims

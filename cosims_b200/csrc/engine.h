@@ -16,7 +16,10 @@
 //     (sigma^6, 24 eps/mu) and uint16 cluster ids as separate arrays, so lanes
 //     reading consecutive atoms hit consecutive banks; ClusterF32 records (FP64
 //     centre and squared radii, so the near/far tests stay FP64; FP32
-//     multipole moments).
+//     multipole moments).  The atom arrays are padded to n_slots, a multiple
+//     of kSlotQuantum, with inert atoms (far away, q = sigma^6 = eps = 0,
+//     cluster id n_clusters, whose mode is always 0): every pair term of a pad
+//     atom is exactly zero, so the pair loop needs no bounds test.
 #pragma once
 #include <cstdint>
 #include "cosims_cuda.h"
@@ -26,6 +29,13 @@ namespace cosims {
 constexpr int kMaxAtoms = 16384;
 constexpr int kMaxClusters = 65535;
 constexpr int kMaxGroupLanes = 32;
+constexpr int kSlotQuantum = 2 * kMaxGroupLanes;   // pair loop: two atoms per lane per pass
+constexpr float kPadCoord = 1.0e6f;                // pad atoms sit this far out (Angstrom)
+constexpr int kMixedMaxBlock = 768;                // threads per CTA of the mixed kernels (80 registers)
+constexpr int kBatchMaxBlock = 768;                // threads per CTA of the batched kernel
+constexpr int kTrajStateBytes = 200;               // one trajectory's integrator state
+constexpr int kGroupStateBytes = 240;              // TrajState + a group's counters (shared memory)
+constexpr int kWideSlotFloats = 24;                // per-warp reduction slot of a wide group
 
 enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_LJ, S_CID, S_COUNT };
 
@@ -66,6 +76,7 @@ struct MolImage {
   int32_t n_atoms;
   int32_t n_clusters;
   int32_t uses_clusters;        // force variant walks clusters (1, 2, 3, 5)
+  int32_t n_slots;              // F32 image: padded atom count (F64 image: n_atoms)
   uint32_t off[S_COUNT];        // byte offsets of the sections (0 = absent)
 };
 
@@ -91,9 +102,57 @@ enum Counter : int {
   C_PAIR_ES,        // electrostatic (+LJ) pair terms
   C_PAIR_POT,       // potential pair terms
   C_FAR,            // far-field cluster terms
-  C_ERROR,          // error flags (bit 0: staging wait gave up)
+  C_ERROR,          // error flags (bit 0: staging wait gave up; bit 1: hand-off wait gave up)
+  C_T_START_INV,    // ~(earliest CTA start), globaltimer ns (max of complements)
+  C_T_DRAIN_INV,    // ~(first time a group found the work queue empty)
+  C_T_END,          // last group exit, globaltimer ns
+  C_WIDE_STEPS,     // steps integrated by wide (hand-off) groups
+  C_WIDE_NS,        // time wide groups spent integrating, summed over groups (ns)
   C_COUNT
 };
+
+// Integrator state of one mixed-form trajectory: in shared memory while a
+// group works on it, in global memory while it waits for a wide group.
+struct TrajState {
+  double pos[3], vel[3], acc[3], p0[3], v0[3];
+  double E0, dt, tries, max_tries, rdot;
+  int64_t t, total;
+  int32_t orbits, step, phase, etries, otries, may_handoff;
+};
+static_assert(sizeof(TrajState) == kTrajStateBytes, "TrajState layout");
+
+// Hand-off of long trajectories (mixed form).  A narrow group (<= 32 lanes)
+// that has integrated `budget` steps of a trajectory parks its state in
+// `states` and takes new work; once a CTA's narrow groups have run out of
+// work, the CTA splits into wide groups of `wide_lanes` threads that finish
+// the parked trajectories.  Every choice is a function of the trajectory, so
+// results do not depend on timing; they do depend on budget and wide_lanes
+// (the order of the FP32 sums changes with the lane count).
+struct Handoff {
+  TrajState *states;               // cap records
+  uint32_t *ready;                 // cap flags, 0 before the launch
+  unsigned long long *reserve;     // records reserved, 0 before the launch
+  unsigned long long *taken;       // records taken by wide groups, 0 before the launch
+  int64_t cap;
+  int64_t budget;                  // steps before a hand-off; 0 = never
+  int32_t wide_lanes;              // threads of a wide group (multiple of 32)
+  int32_t pad;
+};
+
+// Shared-memory bytes of one wide group: cluster modes for two steps, then
+// per-warp reduction slots for two steps (2 x warps x 24 floats, 2 x warps x
+// 4 doubles) and a broadcast word.  The wide group's trajectory state lives in
+// registers.
+__host__ __device__ inline uint32_t wide_group_bytes(int wide_lanes, int mode_stride) {
+  const uint32_t warps = (uint32_t)wide_lanes / 32u;
+  uint32_t b = (2u * (uint32_t)mode_stride + 15u) & ~15u;
+  b += 2u * warps * kWideSlotFloats * 4u;
+  b += 2u * warps * 4u * 8u;
+  b += 16u;
+  return b;
+}
+constexpr int64_t kDefaultHandoffBudget = 1024;   // steps before a trajectory goes wide
+inline int default_wide_lanes(int n_atoms) { return n_atoms <= 1024 ? 128 : 256; }
 
 struct TrajArgs {
   MolImage img;          // the image staged into shared memory
@@ -111,6 +170,7 @@ struct TrajArgs {
   cosims_traj_out *out;  // n records
   unsigned long long *queue;     // work counter (reset to 0 before launch)
   unsigned long long *counters;  // C_COUNT counters
+  Handoff ho;            // mixed form: long-trajectory hand-off (budget 0: off)
 };
 
 // ---- batched form ---------------------------------------------------------------

@@ -124,32 +124,9 @@ extern "C" cosims_status cosims_run_list_noalloc(const cosims_molecule *mol,
   img.gbase = plain ? img64 : img32;
   MolImage i64 = h64.img;
   i64.gbase = img64;
-  int block = plain ? 128 : 256;
-  int mode_stride = 0;
-  if (!plain && img.uses_clusters) {
-    mode_stride = (img.n_clusters + 3) & ~3;
-    if (((mode_stride / 4) & 1) == 0) mode_stride += 4;
-  }
-  const int budget = max_smem - 1024;
-  int use_smem = (int)img.bytes <= budget ? 1 : 0;
-  size_t smem = 0;
-  for (;;) {
-    smem = (use_smem ? img.bytes : 0) + (size_t)(block / G) * mode_stride;
-    if ((int)smem <= budget) break;
-    if (use_smem && block <= (G > 32 ? G : 32)) { use_smem = 0; continue; }
-    if (block <= (G > 32 ? G : 32))
-      return fail(COSIMS_ERR_UNSUPPORTED, "molecule image does not fit in shared memory");
-    block /= 2;
-  }
-  int per_sm = 1;
-  rc = plain ? plain_occupancy(block, smem, &per_sm)
-             : mixed_occupancy(par->force_type, block, smem, &per_sm);
-  if (rc != 0) return cuda_fail((cudaError_t)rc, "occupancy query");
-  if (per_sm < 1) per_sm = 1;
-  const int64_t groups = block / G;
-  int64_t grid = (int64_t)per_sm * sm;
-  if (grid > (n + groups - 1) / groups) grid = (n + groups - 1) / groups;
-  if (grid < 1) grid = 1;
+  LaunchShape ls;
+  cosims_status shs = shape_for(plain, img, G, plain ? 128 : 0, 0, par->force_type, sm, max_smem, n, ls);
+  if (shs != COSIMS_OK) return shs;
 
   TrajArgs a;
   std::memset(&a, 0, sizeof a);
@@ -157,8 +134,8 @@ extern "C" cosims_status cosims_run_list_noalloc(const cosims_molecule *mol,
   a.img64 = i64;
   a.par = dp;
   a.group_lanes = G;
-  a.use_smem = use_smem;
-  a.mode_stride = mode_stride;
+  a.use_smem = ls.use_smem;
+  a.mode_stride = ls.mode_stride;
   a.pos0 = d_pos0;
   a.vel0 = d_vel0;
   a.hit = nullptr;
@@ -167,8 +144,8 @@ extern "C" cosims_status cosims_run_list_noalloc(const cosims_molecule *mol,
   a.out = d_out;
   a.queue = queue;
   a.counters = counters;
-  rc = plain ? plain_launch(a, block, (int)grid, smem, stream)
-             : mixed_launch(a, block, (int)grid, smem, stream);
+  rc = plain ? plain_launch(a, ls.block, ls.grid, ls.smem, stream)
+             : mixed_launch(a, ls.block, ls.grid, ls.smem, stream);
   if (rc != 0) return cuda_fail((cudaError_t)rc, "trajectory kernel launch");
   return COSIMS_OK;
 }

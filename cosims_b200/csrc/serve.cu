@@ -24,7 +24,7 @@ int tuned_group_lanes(int type, int n_atoms);   // batch.cu
 
 namespace {
 
-constexpr int kServeBlock = 256;
+constexpr int kServeBlock = kBatchMaxBlock;
 constexpr uint32_t kServeImageCap = 96 * 1024;
 
 struct Job {
@@ -214,19 +214,10 @@ cosims_status cosims_serve_step(cosims_server *s, void *stream, int32_t *n_finis
     bm.base = base;
     bm.n_traj = std::min<int64_t>(s->round_traj, j.max_traj - j.done);
     bm.first_index = j.done;
-    bm.use_smem = bm.img32.bytes <= kServeImageCap ? 1 : 0;
-    bm.mode_stride = 0;
-    if (bm.img32.uses_clusters) {
-      int m = (bm.img32.n_clusters + 3) & ~3;
-      if (((m / 4) & 1) == 0) m += 4;
-      bm.mode_stride = m;
-    }
-    size_t need = (bm.use_smem ? bm.img32.bytes : 0) +
-                  (size_t)(kServeBlock / bm.group_lanes) * bm.mode_stride;
-    if ((int)need > budget) {
-      bm.use_smem = 0;
-      need = (size_t)(kServeBlock / bm.group_lanes) * bm.mode_stride;
-    }
+    const size_t need = batch_mol_smem(bm, kServeBlock, budget, kServeImageCap);
+    if ((int)need > budget)
+      return fail(COSIMS_ERR_UNSUPPORTED, "job %lld needs %zu bytes of shared memory",
+                  (long long)j.id, need);
     smem = std::max(smem, need);
     const int64_t per = (int64_t)(kServeBlock / bm.group_lanes) * 16;
     for (int64_t t0 = 0; t0 < bm.n_traj; t0 += per) {

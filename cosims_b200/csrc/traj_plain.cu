@@ -368,6 +368,7 @@ __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
     }
     base = smem;
   }
+  if (threadIdx.x == 0) mark_first(a.counters, C_T_START_INV);
   const View m = make_view(base, a.img);
   const DevParams &p = a.par;
   const long long cap = p.max_steps > 0 ? p.max_steps : kDefaultMaxSteps;
@@ -393,7 +394,11 @@ __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
     if (phase == P_ACQUIRE) {
       for (;;) {
         t = (long long)atomicAdd(a.queue, 1ull);
-        if (t >= a.n) { phase = P_DONE; break; }
+        if (t >= a.n) {
+          if (t == a.n) mark_first(a.counters, C_T_DRAIN_INV);   // first to find it empty
+          phase = P_DONE;
+          break;
+        }
         if (a.order) t = a.order[t];
         if (a.hit && !a.hit[t]) {                 // ellipsoid miss: chi = 0
           cosims_traj_out o = {0.0, 0.0, 0, 0u};
@@ -494,6 +499,7 @@ __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
   count_add(c, C_PAIR_ES, w.es);
   count_add(c, C_PAIR_POT, w.pot);
   count_add(c, C_FAR, w.far);
+  if ((threadIdx.x & 31) == 0) mark_last(c, C_T_END);
 }
 
 }  // namespace plain

@@ -66,6 +66,10 @@ def lib():
                 "cosims_batch_set_update_every": (st, [V, C.c_int64]),
                 "cosims_batch_counters": (st, [V, P(abi.CcsSums), P(C.c_float)]),
                 "cosims_ctx_kernel_ms": (st, [V, P(C.c_float)]),
+                "cosims_ctx_kernel_timeline": (st, [V, P(C.c_double), P(C.c_double)]),
+                "cosims_ctx_set_handoff": (st, [V, C.c_int64, C.c_int32]),
+                "cosims_ctx_get_handoff": (st, [V, P(C.c_int64), P(C.c_int32), P(C.c_int64),
+                                                P(C.c_int64), P(C.c_double)]),
                 "cosims_serve_create": (st, [C.c_int32, C.c_int64, C.c_int32, C.c_int64, P(V)]),
                 "cosims_serve_destroy": (None, [V]),
                 "cosims_serve_submit": (st, [V, P(abi.Molecule), P(abi.Params), C.c_uint64,
@@ -183,6 +187,26 @@ class Context:
         ms = C.c_float()
         check(lib().cosims_ctx_kernel_ms(self._h, C.byref(ms)))
         return ms.value
+
+    def set_handoff(self, step_budget: int = 0, wide_lanes: int = 0) -> None:
+        """Mixed form: park trajectories after step_budget steps (0 default,
+        < 0 off) and finish them in wide groups of wide_lanes threads."""
+        check(lib().cosims_ctx_set_handoff(self._h, int(step_budget), int(wide_lanes)))
+
+    def get_handoff(self) -> tuple:
+        """(step_budget, wide_lanes, parked, wide_steps, wide_ms) of the last run."""
+        b, w, n = C.c_int64(), C.c_int32(), C.c_int64()
+        ws, wm = C.c_int64(), C.c_double()
+        check(lib().cosims_ctx_get_handoff(self._h, C.byref(b), C.byref(w), C.byref(n),
+                                           C.byref(ws), C.byref(wm)))
+        return b.value, w.value, n.value, ws.value, wm.value
+
+    def kernel_timeline(self) -> tuple:
+        """(drain_ms, end_ms) of the last trajectory kernel: when a group first
+        found the work queue empty, and when the last group exited."""
+        d, e = C.c_double(), C.c_double()
+        check(lib().cosims_ctx_kernel_timeline(self._h, C.byref(d), C.byref(e)))
+        return d.value, e.value
 
     def sample_inputs(self, seed: int, first: int, n: int, stream=None):
         ins = np.zeros(n, abi.TRAJ_IN_DTYPE)

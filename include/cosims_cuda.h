@@ -177,11 +177,27 @@ cosims_status cosims_ctx_create(const cosims_molecule *mol, const cosims_params 
 void cosims_ctx_destroy(cosims_ctx *ctx);
 
 /* Launch shape: lanes per trajectory (1,2,4,...,32; the plain form accepts 1
- * only) and threads per CTA.  0 keeps the current choice. */
+ * only) and threads per CTA (plain: up to 128; mixed: up to 768, by default
+ * chosen per run for the most resident threads).  0 keeps the current choice.
+ * get_launch reports the CTA size of the last run when it was chosen. */
 cosims_status cosims_ctx_set_launch(cosims_ctx *ctx, int32_t group_lanes,
                                     int32_t block_threads);
 cosims_status cosims_ctx_get_launch(const cosims_ctx *ctx, int32_t *group_lanes,
                                     int32_t *block_threads);
+
+/* Long-trajectory hand-off of the mixed form.  A trajectory still running
+ * after step_budget integration steps (all attempts) is parked and finished
+ * by a wide group of wide_lanes threads once SMs run out of other work, so
+ * the few very long trajectories no longer set the run time.  Results depend
+ * only on the trajectory, group_lanes, step_budget and wide_lanes, not on
+ * timing.  step_budget: 0 = default (1024), < 0 = off; wide_lanes: 0 =
+ * default (128 up to 1024 atoms, else 256), else a multiple of 32 up to 512. */
+cosims_status cosims_ctx_set_handoff(cosims_ctx *ctx, int64_t step_budget, int32_t wide_lanes);
+/* Current settings and, for the last run: trajectories parked, steps the
+ * wide groups integrated, and the time they spent on it summed over wide
+ * groups (ms); wide_ms / wide_steps is the wide groups' time per step. */
+cosims_status cosims_ctx_get_handoff(cosims_ctx *ctx, int64_t *step_budget, int32_t *wide_lanes,
+                                     int64_t *parked, int64_t *wide_steps, double *wide_ms);
 
 /* Fixed-list form: integrate n given start states (pos0, vel0: 3n doubles each,
  * host memory) and write n results to out (host).  Replaces, per trajectory,
@@ -224,6 +240,11 @@ cosims_status cosims_sample_inputs(cosims_ctx *ctx, uint64_t seed, int64_t first
  * events recorded around the launch on its stream; waits for the launch to
  * finish.  No counterpart in the reference: it exists for measurement. */
 cosims_status cosims_ctx_kernel_ms(cosims_ctx *ctx, float *ms);
+/* Timeline of the last trajectory kernel of the context (device clock):
+ * drain_ms = from the first CTA's start until a group first found the work
+ * queue empty; end_ms = until the last group exited.  end_ms - drain_ms is the
+ * tail in which some SMs run out of trajectories.  Synchronises. */
+cosims_status cosims_ctx_kernel_timeline(cosims_ctx *ctx, double *drain_ms, double *end_ms);
 
 /* Measured FMA throughput (TFLOP/s, FMA = 2 flops) of the FP32 and FP64
  * vector pipes of `device`; either output may be NULL.  No counterpart in the

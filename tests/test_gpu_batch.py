@@ -60,7 +60,7 @@ def test_batch_autotune_and_graph_replay():
         b.autotune()
         for m in range(k):
             g, item = b.launch(m)
-            assert g in (2, 4, 8, 16, 32) and item == (256 // g) * 16
+            assert g in (2, 4, 8, 16, 32) and item == (768 // g) * 16   # 768-thread CTAs
         seeds, first, n = np.arange(k) + 1, np.zeros(k, np.int64), np.full(k, 2000)
         r1 = b.run(seeds, first, n)
         r2 = b.run(seeds, first, n)          # replays the captured graph
