@@ -191,9 +191,9 @@ def roofline_traffic():
 def autotune(ctx, stream, torch, d_sums) -> int:
     """Lanes per trajectory for this molecule: the fastest of a short sweep."""
     best, best_ms = None, 1e30
-    for g in (2, 4, 8, 16, 32):
+    for g in (4, 8, 16, 32):
         ctx.set_launch(group_lanes=g)
-        ctx.run_sampled_device(SEED + 7, 0, 20000, 0, d_sums.data_ptr(), stream)
+        ctx.run_sampled_device(SEED + 7, 0, N_TRAJ, 0, d_sums.data_ptr(), stream)
         ms = ctx.kernel_ms()
         if ms < best_ms:
             best, best_ms = g, ms
@@ -218,6 +218,267 @@ def profile_case(args, mol, par, stream, torch) -> None:
                           "last_kernel_ms": ms}))
 
 
+# ---- the batched and serving workloads (configurations 3 and 4) -------------------
+
+def _gen_config3(args_):
+    i, n = args_
+    from cosims_b200 import synth
+    return synth.config3_molecule(i, int(n))
+
+
+def config3_library(n_mol: int, seed: int = 3000):
+    """The synthetic library of the batched configuration: n_mol molecules
+    with log-normal atom counts (median 400, sigma_ln 0.9, 50..5000), charge
+    0..+12 growing as N^(2/3), generated in a spawn pool of host processes."""
+    import multiprocessing as mp
+    from concurrent.futures import ProcessPoolExecutor
+    from cosims_b200 import synth
+    sizes = synth.config3_sizes(max(n_mol, 256), seed)[:n_mol]
+    work = list(enumerate(sizes))
+    work_sorted = sorted(work, key=lambda x: -x[1])            # big ones first
+    with ProcessPoolExecutor(max_workers=max(1, min(cores(), 32)),
+                             mp_context=mp.get_context("spawn")) as ex:
+        mols = dict(zip([i for i, _ in work_sorted], ex.map(_gen_config3, work_sorted)))
+    return [mols[i] for i in range(n_mol)], sizes
+
+
+def setup_library(mols, device: int):
+    """Reference setup of each molecule (boundary ray march on the GPU).
+    Force variant: the LJ cut-off (3 charged / 5 neutral) up to 2000 atoms,
+    the 12 A multipole cut-off (variant 1) above."""
+    from cosims_b200 import host, synth
+    tmp = tempfile.mkdtemp(prefix="cosims_lib_")
+    out = []
+    t0 = time.time()
+    for m in mols:
+        force = "multipole12" if m.n_atoms > 2000 else "cutoff"
+        mp_, ip = synth.write_case(tmp, m, force)
+        st = host.setup_from_files(mp_, ip, seed=SEED, device=device)
+        out.append((st.mol, st.params))
+    shutil.rmtree(tmp, ignore_errors=True)
+    return out, time.time() - t0
+
+
+def batched_workload(args, rank, world, local, dist, torch):
+    """Configuration 3: 256 molecules x 2e4 trajectories in one persistent
+    launch (device work queue, CUDA graph, autotuned lanes per trajectory),
+    against per-molecule plain FP64 launches timed on a stratified subset."""
+    import numpy as np
+    from cosims_b200 import abi, engine
+    per_mol = 20000
+    t0 = time.time()
+    mols, sizes = config3_library(args.molecules)
+    gen_s = time.time() - t0
+    lib_, setup_s = setup_library(mols, local)
+    ms_, pars = [m for m, _ in lib_], [p for _, p in lib_]
+    k = len(ms_)
+    stream = torch.cuda.current_stream()
+    seeds = np.arange(k, dtype=np.uint64) + np.uint64(SEED)
+    n = np.full(k, per_mol, np.int64)
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    b = engine.Batch(ms_, pars, device=local)
+    t1 = time.time()
+    b.autotune()
+    tune_s = time.time() - t1
+    first0 = rank * 10 ** 9
+    for w in range(args.warmup):
+        b.run(seeds, np.full(k, first0 + w * per_mol, np.int64), n)
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    step_ms, kern_ms, sums_all = [], [], []
+    for s_ in range(args.steps):
+        flush.zero_()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        sums = b.run(seeds, np.full(k, first0 + (args.warmup + s_) * per_mol, np.int64), n,
+                     stream)
+        e.record(stream)
+        torch.cuda.synchronize()
+        step_ms.append(a.elapsed_time(e))
+        work, kms = b.counters()
+        kern_ms.append(kms)
+        sums_all.append(sums)
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    mean_ms = sum(step_ms) / len(step_ms)
+    if dist:
+        t = torch.tensor([mean_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        mean_ms = float(t.item())
+    total = int(n.sum())
+    value = world * total / (mean_ms / 1000.0)
+    flops = FLOPS_LJ * work.pair_lj + FLOPS_ES * work.pair_es + FLOPS_FAR * work.far_terms + \
+        FLOPS_POT_CHARGED * work.pair_pot
+    fp32_peak, _ = engine.probe_peaks(local)
+    achieved = flops / (kern_ms[-1] / 1000.0) / 1e12
+
+    # plain FP64, one launch per molecule, on every 16th molecule by size
+    order = np.argsort(sizes)
+    subset = [int(i) for i in order[::max(1, k // 16)]]
+    first_cmp = first0 + args.warmup * per_mol
+    ref = sums_all[0]
+    plain_ms, errs, mixed_ms = 0.0, [], 0.0
+    d = torch.zeros(1024, dtype=torch.uint8, device="cuda")
+    sz = abi.C.sizeof(abi.CcsSums)
+    for i in subset:
+        with engine.Context(ms_[i], pars[i], abi.PLAIN_F64, device=local) as pc:
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            pc.run_sampled_device(int(seeds[i]), first_cmp, per_mol, 0, d.data_ptr(), stream)
+            e.record(stream)
+            torch.cuda.synchronize()
+            plain_ms += a.elapsed_time(e)
+            ps = abi.CcsSums.from_buffer_copy(d.cpu().numpy()[:sz].tobytes())
+        errs.append(abs(ref[i].sum - ps.sum) / ps.sum * 100.0)
+        with engine.Context(ms_[i], pars[i], abi.MIXED, device=local) as mc:
+            mc.set_launch(group_lanes=b.launch(i)[0])
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            mc.run_sampled_device(int(seeds[i]), first_cmp, per_mol, 0, d.data_ptr(), stream)
+            e.record(stream)
+            torch.cuda.synchronize()
+            mixed_ms += a.elapsed_time(e)
+    scale = k / len(subset)
+    plain_value = total / (plain_ms * scale / 1000.0)
+    # the subset is stratified by size: scale its time to the 256 molecules
+    b.close()
+    if rank == 0:
+        types = sorted({int(p.force_type) for p in pars})
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 pair forces / fp64 integration", "data": "synthetic",
+            "config": {"workload": f"batched: {k} synthetic molecules (atoms log-normal, median "
+                                   f"400, 50..5000; charge 0..+12) x {per_mol} trajectories, "
+                                   "one persistent launch per step (CUDA graph)",
+                       "molecules": k, "atoms_total": int(sizes.sum()),
+                       "atoms_median": int(np.median(sizes)), "atoms_max": int(sizes.max()),
+                       "force_types": types, "traj_per_step": total,
+                       "l2": "flushed between steps (512 MiB write)"},
+            "ccs": {"err_pct_batched_mixed_vs_plain": {"max": max(errs),
+                                                        "mean": sum(errs) / len(errs),
+                                                        "molecules": len(subset)},
+                    "bar_pct": 0.3},
+            "plain_f64_per_molecule_launches": {
+                "value": plain_value, "unit": UNIT,
+                "estimate": f"{len(subset)} molecules (every {k // len(subset)}th by size) "
+                            f"x {per_mol} trajectories, time scaled by {scale:g}"},
+            "mixed_per_molecule_launches": {"value": total / (mixed_ms * scale / 1000.0),
+                                            "unit": UNIT},
+            "batched_over_plain": value / world / plain_value,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                         "kernel": "batch_mixed_kernel", "kernel_ms": kern_ms[-1]},
+            "host_s": {"generate": round(gen_s, 1), "setup": round(setup_s, 1),
+                       "autotune": round(tune_s, 1)},
+            "gpu_launches": 3 * args.steps,   # sample, trajectories, reduce (one graph)
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+
+
+def serving_workload(args, rank, world, local, dist, torch):
+    """Configuration 4: CCS requests arrive as a Poisson stream; each names a
+    molecule of the configuration-3 library and a target relative standard
+    error (0.5 %, or 0.2 % for one request in ten).  Requests are admitted as
+    slots and HBM budget free up, run in rounds through the persistent kernel
+    with everything else in flight, and retire at their target.  Latency is
+    from arrival to retirement; the molecules' host setup is done beforehand
+    and reported apart."""
+    import numpy as np
+    from cosims_b200 import abi, engine
+    if rank != 0:
+        return
+    mols, sizes = config3_library(args.molecules)
+    lib_, setup_s = setup_library(mols, local)
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    n_req = int(args.rate * args.duration * 1.5) + 16
+    gaps = rng.exponential(1.0 / args.rate, size=n_req)
+    arrivals = np.cumsum(gaps)
+    arrivals = arrivals[arrivals < args.duration]
+    which = rng.integers(0, len(lib_), size=len(arrivals))
+    target = np.where(rng.random(len(arrivals)) < 0.1, 0.002, 0.005)
+    round_traj = 8192
+    srv = engine.Server(device=local, hbm_budget=16 << 30, max_jobs=128, round_traj=round_traj)
+    # warm the kernels and the tuning on a few jobs
+    for j in range(4):
+        m, p = lib_[j]
+        jid = srv.submit(m, p, 1 + j, 0.05, min_traj=round_traj, max_traj=4 * round_traj)
+        while srv.poll(jid).state == abi.JOB_RUNNING:
+            srv.step()
+        srv.release(jid)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t0 = time.perf_counter()
+    pending, live, done = 0, {}, []
+    traj_done = 0
+    while pending < len(arrivals) or live:
+        now = time.perf_counter() - t0
+        while pending < len(arrivals) and arrivals[pending] <= now:
+            m, p = lib_[int(which[pending])]
+            jid = srv.submit(m, p, SEED + pending, float(target[pending]), min_traj=round_traj,
+                             max_traj=400 * round_traj)
+            if jid is None:
+                break                                    # no room: admit later, in order
+            live[jid] = pending
+            pending += 1
+        if not live:
+            if pending < len(arrivals):
+                time.sleep(max(0.0, min(0.01, arrivals[pending] - now)))
+            continue
+        srv.step()
+        t_now = time.perf_counter() - t0
+        for jid in list(live):
+            stt = srv.poll(jid)
+            if stt.state == abi.JOB_DONE:
+                r = live.pop(jid)
+                done.append((r, t_now - arrivals[r], stt.omega, stt.rel_se, stt.sums.n,
+                             int(which[r]), float(target[r])))
+                traj_done += stt.sums.n
+                srv.release(jid)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    lat = np.array([d_[1] for d_ in done])
+    # CCS of a small sample against the plain FP64 form on the same trajectories
+    sample = done[:: max(1, len(done) // 3)][:3]
+    errs = []
+    d = torch.zeros(1024, dtype=torch.uint8, device="cuda")
+    sz = abi.C.sizeof(abi.CcsSums)
+    for (r, _, om, _, ntr, mi, _) in sample:
+        m, p = lib_[mi]
+        with engine.Context(m, p, abi.PLAIN_F64, device=local) as pc:
+            pc.run_sampled_device(SEED + r, 0, int(ntr), 0, d.data_ptr(),
+                                  torch.cuda.current_stream())
+            ps = abi.CcsSums.from_buffer_copy(d.cpu().numpy()[:sz].tobytes())
+        errs.append(abs(om - ps.sum / ps.n_eff) / (ps.sum / ps.n_eff) * 100.0)
+    srv.close()
+    line = {
+        "metric": METRIC, "value": traj_done / wall, "unit": UNIT, "n_gpus": 1,
+        "steps": len(done), "warmup": 4, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32 pair forces / fp64 integration", "data": "synthetic",
+        "config": {"workload": f"serving: Poisson arrivals at {args.rate:g} req/s for "
+                               f"{args.duration:g} s; molecules from a {len(lib_)}-molecule "
+                               "configuration-3 library; target rel. SE 0.5 % (0.2 % for 10 %)",
+                   "round_traj": round_traj, "max_jobs": 128},
+        "requests": {"arrived": int(len(arrivals)), "completed": len(done),
+                     "admitted": int(pending), "per_s": len(done) / wall,
+                     "wall_s": wall},
+        "latency_s": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
+                      "p99": float(np.percentile(lat, 99)) if len(lat) else None,
+                      "max": float(lat.max()) if len(lat) else None},
+        "ccs": {"err_pct_vs_plain_f64": errs, "sample": len(errs), "bar_pct": 0.3},
+        "host_setup_s_per_molecule": setup_s / len(lib_),
+        "clocks": clk,
+    }
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -230,6 +491,12 @@ def main():
                          "of one form only, no L2 flush buffer, no sweep")
     ap.add_argument("--profile-traj", type=int, default=20000)
     ap.add_argument("--group-lanes", type=int, default=0)
+    ap.add_argument("--workload", choices=["integral", "batched", "serving"], default="integral",
+                    help="integral: the 512-atom ion (default line); batched: 256 molecules "
+                         "in one persistent launch; serving: Poisson stream of CCS requests")
+    ap.add_argument("--molecules", type=int, default=256, help="batched/serving: library size")
+    ap.add_argument("--rate", type=float, default=50.0, help="serving: requests per second")
+    ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -249,6 +516,12 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local))
     from cosims_b200 import abi, engine, host
+    if args.workload == "batched":
+        batched_workload(args, rank, world, local, dist, torch)
+        return
+    if args.workload == "serving":
+        serving_workload(args, rank, world, local, dist, torch)
+        return
 
     tmp = tempfile.mkdtemp(prefix="cosims_bench_")
     _, mp, ip = workload_files(tmp)
@@ -278,6 +551,7 @@ def main():
           for _ in range(args.steps)]
     kern_ms = []
     sz = abi.C.sizeof(abi.CcsSums)
+    tails, parked = [], []
     for k in range(args.steps):
         flush.zero_()                                   # L2 flush between steps
         ev[k][0].record(stream)
@@ -285,6 +559,9 @@ def main():
                                step_sums[k].data_ptr(), stream)
         ev[k][1].record(stream)
         kern_ms.append(ctx.kernel_ms())
+        drain, end = ctx.kernel_timeline()
+        tails.append((drain, end))
+        parked.append(ctx.get_handoff()[2])
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -368,6 +645,7 @@ def main():
                "sample": f"one integral of {traj} trajectories of the same molecule and "
                          f"input (reference program, OpenMP threads = {nc})"}
 
+    ho = ctx.get_handoff()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -394,6 +672,10 @@ def main():
                             "per-trajectory records"},
             "gpu_launches": 7 * args.steps,   # sample, 3 x work order, trajectories, 2 x reduce
             "clocks": clk,
+            "tail": {"queue_drained_ms": [round(a, 2) for a, _ in tails],
+                     "kernel_end_ms": [round(b, 2) for _, b in tails],
+                     "handoff": {"step_budget": ho[0], "wide_lanes": ho[1],
+                                 "parked_per_step": parked}},
         }
         print(json.dumps(line))
     ctx.close()

@@ -274,37 +274,43 @@ cosims_status shape_for(bool plain, const MolImage &img, int G, int block_thread
   bool found = false;
   int best_resident = -1;
   for (int ci = 0; ci < ncand; ci++) {
-    int block = cands[ci];
-    if (block < G) continue;
-    LaunchShape t;
-    t.use_smem = (int)img_bytes <= budget ? 1 : 0;
-    t.mode_stride = stride;
-    // shrink the CTA until image + group scratch fit
-    bool ok = true;
-    for (;;) {
-      size_t scratch = (size_t)(block / G) * per_group;
-      // wide phase: whole wide groups only, at most 15 (named barriers 1..15)
-      t.wide_lanes = (per_wide && block >= wide_lanes && block / wide_lanes <= 15) ? wide_lanes : 0;
-      if (t.wide_lanes) scratch = std::max(scratch, (size_t)(block / wide_lanes) * per_wide);
-      size_t smem = (t.use_smem ? img_bytes : 0) + scratch;
-      if ((int)smem <= budget) { t.smem = smem; break; }
-      if (t.use_smem && block <= std::max(G, 32)) { t.use_smem = 0; continue; }
-      if (block <= std::max(G, 32)) { ok = false; break; }
-      block /= 2;
-    }
-    if (!ok) continue;
-    t.block = block;
-    int per_sm = 0;
-    int rc = plain ? plain_occupancy(block, t.smem, &per_sm)
-                   : mixed_occupancy(force_type, t.use_smem, block, t.smem, &per_sm);
-    if (rc != 0) return cuda_fail((cudaError_t)rc, "occupancy query");
-    if (per_sm <= 0) continue;          // over the kernel's thread or register limit
-    const int resident = per_sm * block * (t.use_smem ? 2 : 1);
-    if (resident > best_resident) {
-      best_resident = resident;
-      t.grid = per_sm;                  // CTAs per SM until the grid is sized below
-      ls = t;
-      found = true;
+    for (int staged = 1; staged >= 0; staged--) {   // staged image first, then read from L2
+      int block = cands[ci];
+      if (block < G) continue;
+      if (staged && (int)img_bytes > budget) continue;
+      LaunchShape t;
+      t.use_smem = staged;
+      t.mode_stride = stride;
+      // shrink the CTA until image + group scratch fit
+      bool ok = true;
+      for (;;) {
+        size_t scratch = (size_t)(block / G) * per_group;
+        // wide phase: whole wide groups only, at most 15 (named barriers 1..15)
+        t.wide_lanes = (per_wide && block >= wide_lanes && block / wide_lanes <= 15) ? wide_lanes : 0;
+        if (t.wide_lanes) scratch = std::max(scratch, (size_t)(block / wide_lanes) * per_wide);
+        size_t smem = (t.use_smem ? img_bytes : 0) + scratch;
+        if ((int)smem <= budget) { t.smem = smem; break; }
+        if (block <= std::max(G, 32)) { ok = false; break; }
+        block /= 2;
+      }
+      if (!ok) continue;
+      t.block = block;
+      int per_sm = 0;
+      int rc = plain ? plain_occupancy(block, t.smem, &per_sm)
+                     : mixed_occupancy(force_type, t.use_smem, block, t.smem, &per_sm);
+      if (rc != 0) {
+        cudaGetLastError();             // a refused shared-memory size: try the next shape
+        continue;
+      }
+      if (per_sm <= 0) continue;        // over the kernel's thread, register or smem limit
+      const int resident = per_sm * block * (t.use_smem ? 2 : 1);
+      if (resident > best_resident) {
+        best_resident = resident;
+        t.grid = per_sm;                // CTAs per SM until the grid is sized below
+        ls = t;
+        found = true;
+      }
+      if (per_sm > 0) break;            // staged works: no need to try unstaged
     }
   }
   if (!found) return fail(COSIMS_ERR_UNSUPPORTED, "molecule image does not fit in shared memory");

@@ -66,8 +66,27 @@ def composition_counts(ratios: dict, n: int) -> dict:
 
 
 def random_walk(n: int, r_ball: float, rng: np.random.Generator) -> np.ndarray:
-    """Self-avoiding walk of n atoms from the origin inside a ball of radius r_ball."""
+    """Self-avoiding walk of n atoms from the origin inside a ball of radius r_ball.
+
+    Candidate directions come TRIES at a time; the first one inside the ball
+    and at least MIN_SEP from every placed atom is taken, else the tip backs
+    up along the chain.  Placed atoms are binned in cells of side MIN_SEP, so
+    the separation test reads only the 27 cells around a candidate (the same
+    distances, hence the same walk, as a test against every atom)."""
     xyz = np.zeros((n, 3))
+    cap = 8                                   # atoms MIN_SEP apart: at most 8 per cell
+    nc = int(math.ceil(2.0 * (r_ball + STEP) / MIN_SEP)) + 3
+    grid = np.full((nc, nc, nc, cap), -1, dtype=np.int64)
+    fill = np.zeros((nc, nc, nc), dtype=np.int64)
+    off = (nc // 2)
+    nbr = np.array([(i, j, k) for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)])
+
+    def cell_of(p):
+        return np.floor(p / MIN_SEP).astype(np.int64) + off
+
+    c0 = cell_of(xyz[0])
+    grid[c0[0], c0[1], c0[2], 0] = 0
+    fill[c0[0], c0[1], c0[2]] = 1
     tip = 0
     count = 1
     guard = 0
@@ -80,12 +99,23 @@ def random_walk(n: int, r_ball: float, rng: np.random.Generator) -> np.ndarray:
         cand = xyz[tip] + STEP * d
         ok = np.linalg.norm(cand, axis=1) <= r_ball
         if ok.any():
-            diff = cand[:, None, :] - xyz[None, :count, :]
-            dmin = np.sqrt((diff * diff).sum(axis=2)).min(axis=1)
-            ok &= dmin >= MIN_SEP
+            cells = cell_of(cand)[:, None, :] + nbr[None, :, :]          # (T, 27, 3)
+            ids = grid[cells[..., 0], cells[..., 1], cells[..., 2]]      # (T, 27, cap)
+            ids = ids.reshape(TRIES, -1)
+            valid = ids >= 0
+            diff = cand[:, None, :] - xyz[np.where(valid, ids, 0)]
+            dist = np.sqrt((diff * diff).sum(axis=2))
+            dist = np.where(valid, dist, np.inf)
+            ok &= dist.min(axis=1) >= MIN_SEP
         idx = np.flatnonzero(ok)
         if idx.size:
             xyz[count] = cand[idx[0]]
+            c = cell_of(xyz[count])
+            f = fill[c[0], c[1], c[2]]
+            if f >= cap:
+                raise RuntimeError("cell capacity exceeded")
+            grid[c[0], c[1], c[2], f] = count
+            fill[c[0], c[1], c[2]] = f + 1
             tip = count
             count += 1
         else:
