@@ -386,21 +386,28 @@ cosims_status cosims_batch_autotune(cosims_batch *b, void *stream) {
   std::map<std::pair<int, int>, int> best_g;
   for (auto &kv : rep) {
     const int m = kv.second;
+    const int slots = b->mols[m].img32.n_slots;
     float best = 1e30f;
     int best_lanes = b->mols[m].group_lanes;
+    // about four million pair terms per evaluation run; lanes that leave each
+    // lane between 8 and 256 atom slots (fewer is all overhead, more is all tail)
+    const int64_t trials = std::min<int64_t>(16384, std::max<int64_t>(2048, (4 << 20) / slots));
+    bool warmed = false;
     for (int lanes : {2, 4, 8, 16, 32}) {
-      if (lanes < 4 && b->n_atoms[m] > 256) continue;
+      if (slots / lanes > 256 && lanes != 32) continue;
+      if (slots / lanes < 8 && lanes != 2) continue;
       b->mols[m].group_lanes = lanes;
       if (shape_launch(b) != COSIMS_OK) continue;
       drop_graph(b);
       std::fill(n.begin(), n.end(), 0);
-      n[m] = 4096;
+      n[m] = trials;
       float ms = 0;
       bool ok = true;
-      for (int rep_i = 0; rep_i < 2 && ok; rep_i++) {
+      for (int rep_i = 0; rep_i < (warmed ? 1 : 2) && ok; rep_i++) {
         if (cosims_batch_run(b, seeds.data(), first.data(), n.data(), sums.data(), stream) !=
             COSIMS_OK) ok = false;
       }
+      warmed = true;
       if (!ok) continue;
       cudaEventElapsedTime(&ms, b->ev0, b->ev1);
       if (ms < best) { best = ms; best_lanes = lanes; }

@@ -333,13 +333,18 @@ cosims_status launch_shape(const cosims_ctx *c, int64_t n, LaunchShape &ls) {
                    c->max_smem, n, ls);
 }
 
-// Hand-off buffers for n trajectories: one record per 16 trajectories (at
-// least 256), ready flags and counters cleared on the stream.
+// Hand-off buffers for n trajectories: a record for every trajectory, so a
+// park never fails and which trajectories go wide depends on them alone (a
+// smaller array would fill in timing order).  Above kHandoffMaxRecords
+// trajectories a call runs without hand-off.  Ready flags and counters are
+// cleared on the stream.
+constexpr int64_t kHandoffMaxRecords = 1 << 22;    // 800 MiB of records
+
 cosims_status handoff_prepare(cosims_ctx *c, int64_t n, const LaunchShape &ls, Handoff &ho,
                               cudaStream_t s) {
   std::memset(&ho, 0, sizeof ho);
-  if (!ls.wide_lanes || n == 0) return COSIMS_OK;
-  const int64_t want = std::min<int64_t>(std::max<int64_t>(256, n / 16), 1 << 20);
+  if (!ls.wide_lanes || n == 0 || n > kHandoffMaxRecords) return COSIMS_OK;
+  const int64_t want = std::max<int64_t>(n, 256);
   if (c->ho_cap < want) {
     cudaFree(c->d_ho_states);
     cudaFree(c->d_ho_ready);

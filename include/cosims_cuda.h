@@ -191,7 +191,9 @@ cosims_status cosims_ctx_get_launch(const cosims_ctx *ctx, int32_t *group_lanes,
  * the few very long trajectories no longer set the run time.  Results depend
  * only on the trajectory, group_lanes, step_budget and wide_lanes, not on
  * timing.  step_budget: 0 = default (1024), < 0 = off; wide_lanes: 0 =
- * default (128 up to 1024 atoms, else 256), else a multiple of 32 up to 512. */
+ * default (128 up to 1024 atoms, else 256), else a multiple of 32 up to 512.
+ * The context keeps a 200-byte record per trajectory of a call for this; calls
+ * of more than 2^22 trajectories run without hand-off. */
 cosims_status cosims_ctx_set_handoff(cosims_ctx *ctx, int64_t step_budget, int32_t wide_lanes);
 /* Current settings and, for the last run: trajectories parked, steps the
  * wide groups integrated, and the time they spent on it summed over wide
