@@ -131,16 +131,23 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   const int ns = (n + kSlotQuantum - 1) / kSlotQuantum * kSlotQuantum;
   std::vector<AtomF64> a64(n);
   std::vector<float4> a4(ns, make_float4(kPadCoord, kPadCoord, kPadCoord, 0.0f));
-  std::vector<float2> lj2(ns, make_float2(0.0f, 0.0f));
-  std::vector<uint16_t> cid16(ns, (uint16_t)nc);
+  // second record: sigma^6, 24 eps/mu, cluster id (integer bits), 0; pad atoms
+  // belong to cluster nc, whose mode is always 0
+  std::vector<float4> b4(ns, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+  uint32_t pad_cid = (uint32_t)nc;
+  float pad_cid_f;
+  std::memcpy(&pad_cid_f, &pad_cid, 4);
+  for (int k = n; k < ns; k++) b4[k].z = pad_cid_f;
   for (int k = 0; k < n; k++) {
     const int i = order[k];
     AtomF64 &A = a64[k];
     A.x = m->x[i]; A.y = m->y[i]; A.z = m->z[i]; A.q = m->charge[i];
     A.sig6 = m->sig6[i]; A.eps24m = m->eps24m[i]; A.eps4 = m->eps4[i];
     a4[k] = make_float4((float)A.x, (float)A.y, (float)A.z, (float)A.q);
-    lj2[k] = make_float2((float)A.sig6, (float)A.eps24m);
-    cid16[k] = (uint16_t)cid[k];
+    uint32_t ck = (uint32_t)cid[k];
+    float ck_f;
+    std::memcpy(&ck_f, &ck, 4);
+    b4[k] = make_float4((float)A.sig6, (float)A.eps24m, ck_f, 0.0f);
   }
   std::vector<ClusterF64> c64(nc);
   std::vector<ClusterF32> c32(nc);
@@ -190,8 +197,7 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   MolImage &i32 = h32.img;
   std::memset(&i32, 0, sizeof i32);
   i32.off[S_ATOMS] = b32.add(a4.data(), sizeof(float4) * ns);
-  i32.off[S_LJ] = b32.add(lj2.data(), sizeof(float2) * ns);
-  i32.off[S_CID] = b32.add(cid16.data(), sizeof(uint16_t) * ns);
+  i32.off[S_LJ] = b32.add(b4.data(), sizeof(float4) * ns);
   i32.off[S_CLUSTERS] = b32.add(c32.data(), sizeof(ClusterF32) * nc);
   b32.finish();
   i32.bytes = (uint32_t)b32.buf.size();
@@ -297,7 +303,7 @@ cosims_status shape_for(bool plain, const MolImage &img, int G, int block_thread
       t.block = block;
       int per_sm = 0;
       int rc = plain ? plain_occupancy(block, t.smem, &per_sm)
-                     : mixed_occupancy(force_type, t.use_smem, block, t.smem, &per_sm);
+                     : mixed_occupancy(force_type, t.use_smem, G, block, t.smem, &per_sm);
       if (rc != 0) {
         cudaGetLastError();             // a refused shared-memory size: try the next shape
         continue;

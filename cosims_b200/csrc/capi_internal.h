@@ -39,7 +39,8 @@ struct DeviceGuard {
 };
 
 int plain_occupancy(int block, size_t smem, int *per_sm);
-int mixed_occupancy(int force_type, int use_smem, int block, size_t smem, int *per_sm);
+int mixed_occupancy(int force_type, int use_smem, int group_lanes, int block, size_t smem,
+                    int *per_sm);
 
 // Lanes per trajectory before any tuning: enough lanes that a 32-lane warp
 // still holds several trajectories for small molecules, a full warp for large.

@@ -12,8 +12,8 @@
 //     reference's member order for the cluster force variants (1, 2, 3, 5),
 //     file order otherwise; perm[i] = force-order slot of file atom i
 //     (getPotential walks atoms in file order); ClusterF64 records.
-//   F32 image (mixed form): in force order, float4 (x, y, z, q), float2
-//     (sigma^6, 24 eps/mu) and uint16 cluster ids as separate arrays, so lanes
+//   F32 image (mixed form): in force order, two float4 arrays, (x, y, z, q)
+//     and (sigma^6, 24 eps/mu, cluster id as integer bits, 0), so lanes
 //     reading consecutive atoms hit consecutive banks; ClusterF32 records (FP64
 //     centre and squared radii, so the near/far tests stay FP64; FP32
 //     multipole moments).  The atom arrays are padded to n_slots, a multiple
@@ -37,7 +37,7 @@ constexpr int kTrajStateBytes = 200;               // one trajectory's integrato
 constexpr int kGroupStateBytes = 240;              // TrajState + a group's counters (shared memory)
 constexpr int kWideSlotFloats = 24;                // per-warp reduction slot of a wide group
 
-enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_LJ, S_CID, S_COUNT };
+enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_LJ, S_COUNT };
 
 struct AtomF64 {            // 56 bytes
   double x, y, z, q, sig6, eps24m, eps4;

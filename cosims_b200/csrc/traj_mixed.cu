@@ -1,1058 +1,9 @@
-// traj_mixed.cu -- the mixed-precision form.
-//
-// Pair forces (Lennard-Jones and the ion-induced-dipole field and field
-// gradient) are FP32 on molecule-centred coordinates; the He position enters
-// as an FP32 hi/lo pair, so dx = (x_hi - x_atom) + x_lo keeps the separation
-// accurate to FP32 precision of dx itself at close approach.  FP64 is kept for
-// the position/velocity accumulators of the Verlet step, the cluster near/far
-// tests, the energy-conservation check (exact potential, FP64) and the
-// scattering angle; the CCS sum uses 2 sin^2(chi/2) for 1 - cos(chi).
-//
-// G lanes (1..32) work on one trajectory: they split the atoms, reduce the
-// accumulators with xor-butterfly shuffles (bitwise identical in every lane),
-// and run the integrator redundantly, so the group needs no broadcast.  The
-// physics is the reference's (forceAccel.cpp:221-884), including its
-// multipoleCutoff far band that takes sigma^6/eps of atom index n
-// (forceAccel.cpp:353-355); only the arithmetic precision and the order of the
-// sums differ from the plain form.
-#include <cuda_runtime.h>
-#include "device_util.cuh"
+// traj_mixed.cu -- the batched mixed-form kernel and the dispatch of the
+// single-molecule kernels (compiled per force variant in traj_mixed_t<N>.cu).
+#include "mixed_impl.cuh"
 
 namespace cosims {
 namespace mixed {
-
-enum ModeBits : uint8_t { M_ES = 1, M_LJ = 2, M_LJQ = 4 };
-
-struct View {
-  const float4 *a4;        // x, y, z, q
-  const float2 *lj;        // sigma^6, 24 eps/mu
-  const uint16_t *cid;     // cluster of each atom
-  const ClusterF32 *cl;
-  int n, nc, nslots;        // atoms, clusters, padded atom slots
-};
-
-struct View64 {   // FP64 image in global memory, for the energy check
-  const AtomF64 *at;
-  int n;
-};
-
-__device__ __forceinline__ View make_view(const unsigned char *b, const MolImage &img) {
-  View v;
-  v.a4 = reinterpret_cast<const float4 *>(b + img.off[S_ATOMS]);
-  v.lj = reinterpret_cast<const float2 *>(b + img.off[S_LJ]);
-  v.cid = reinterpret_cast<const uint16_t *>(b + img.off[S_CID]);
-  v.cl = reinterpret_cast<const ClusterF32 *>(b + img.off[S_CLUSTERS]);
-  v.n = img.n_atoms;
-  v.nc = img.n_clusters;
-  v.nslots = img.n_slots;
-  return v;
-}
-
-__device__ __forceinline__ View64 make_view64(const MolImage &img) {
-  View64 v;
-  v.at = reinterpret_cast<const AtomF64 *>(img.gbase + img.off[S_ATOMS]);
-  v.n = img.n_atoms;
-  return v;
-}
-
-struct Acc {
-  float Fx, Fy, Fz;                 // Lennard-Jones force sum
-  float Ex, Ey, Ez;                 // charge field
-  float Pxx, Pxy, Pxz, Pyy, Pyz, Pzz, Q3;   // sum q d d^T / r^5, sum q / r^3
-  float Mdx, Mdy, Mdz, Msxy, Msxz, Msyz, Maxy, Maxz, Mayz;  // far-field gradient
-};
-
-template <int TYPE>
-struct Traits {
-  static constexpr bool kClusters = TYPE == 1 || TYPE == 2 || TYPE == 3 || TYPE == 5;
-  // pair terms per evaluation depend on the position (far clusters, cut-off
-  // without a charge field); for 3, 4 and 6 they are n_atoms every time
-  static constexpr bool kVaryingPairs = TYPE == 1 || TYPE == 2 || TYPE == 5;
-  static constexpr bool kCharge = TYPE <= 4;
-  static constexpr bool kFar = TYPE == 1 || TYPE == 2;
-  // every atom carries the charge field (types 3, 4): no per-pair branch
-  static constexpr bool kEsAlways = TYPE == 3 || TYPE == 4;
-};
-
-// Far-field monopole + dipole (+ quadrupole) terms of one cluster, in FP32,
-// the reference's far block (forceAccel.cpp:258-337).
-__device__ __forceinline__ void far_terms(const View &m, int n, int order, float dx0, float dx1,
-                                          float dx2, Acc &s) {
-  const float xx = dx0 * dx0, yy = dx1 * dx1, zz = dx2 * dx2;
-  const float r2 = xx + yy + zz;
-  const float r_2 = 1.0f / r2;
-  const float r_1 = rsqrtf(r2);
-  const float r_3 = r_2 * r_1;
-  const float r_5 = r_3 * r_2;
-  const float xy = dx0 * dx1, xz = dx0 * dx2, yz = dx1 * dx2;
-  const ClusterF32 &C = m.cl[n];
-  const float cR5 = C.q * r_5;
-  const float cR3 = cR5 * r2;
-  s.Ex += cR3 * dx0; s.Ey += cR3 * dx1; s.Ez += cR3 * dx2;
-  s.Mdx += (r2 - 3.f * xx) * cR5; s.Mdy += (r2 - 3.f * yy) * cR5; s.Mdz += (r2 - 3.f * zz) * cR5;
-  s.Msxy -= 3.f * xy * cR5; s.Msxz -= 3.f * xz * cR5; s.Msyz -= 3.f * yz * cR5;
-  if (order >= 1 && !C.replaced) {
-    const float *D = C.dip;
-    const float r_7 = r_5 * r_2;
-    const float c1 = 3.f * (D[0] * dx0 + D[1] * dx1 + D[2] * dx2);
-    s.Ex += (c1 * dx0 - r2 * D[0]) * r_5;
-    s.Ey += (c1 * dx1 - r2 * D[1]) * r_5;
-    s.Ez += (c1 * dx2 - r2 * D[2]) * r_5;
-    s.Mdx += (r2 - 5.f * xx) * r_7 * c1;
-    s.Mdy += (r2 - 5.f * yy) * r_7 * c1;
-    s.Mdz += (r2 - 5.f * zz) * r_7 * c1;
-    s.Msxy -= 5.f * xy * r_7 * c1; s.Msxz -= 5.f * xz * r_7 * c1; s.Msyz -= 5.f * yz * r_7 * c1;
-    s.Maxy += 3.f * (D[1] * dx0 - D[0] * dx1) * r_5;
-    s.Maxz += 3.f * (D[2] * dx0 - D[0] * dx2) * r_5;
-    s.Mayz += 3.f * (D[2] * dx1 - D[1] * dx2) * r_5;
-  }
-  if (order >= 2) {
-    const float *Q = C.quad;
-    const float r_7 = r_5 * r_2;
-    const float t0 = (Q[0] * dx0 + Q[3] * dx1 + Q[6] * dx2) * r_7;
-    const float t1 = (Q[1] * dx0 + Q[4] * dx1 + Q[7] * dx2) * r_7;
-    const float t2 = (Q[2] * dx0 + Q[5] * dx1 + Q[8] * dx2) * r_7;
-    const float c2 = 5.f * (t0 * dx0 + t1 * dx1 + t2 * dx2) * r_2 * 0.5f;
-    s.Ex += (c2 * dx0 - t0) * r2; s.Ey += (c2 * dx1 - t1) * r2; s.Ez += (c2 * dx2 - t2) * r2;
-    s.Mdx += (r2 - 7.f * xx) * c2 - Q[0] * r_5;
-    s.Mdy += (r2 - 7.f * yy) * c2 - Q[4] * r_5;
-    s.Mdz += (r2 - 7.f * zz) * c2 - Q[8] * r_5;
-    s.Msxy -= 7.f * xy * c2 + Q[1] * r_5;
-    s.Msxz -= 7.f * xz * c2 + Q[2] * r_5;
-    s.Msyz -= 7.f * yz * c2 + Q[5] * r_5;
-    s.Maxy += 5.f * (t1 * dx0 - t0 * dx1);
-    s.Maxz += 5.f * (t2 * dx0 - t0 * dx2);
-    s.Mayz += 5.f * (t2 * dx1 - t1 * dx2);
-  }
-}
-
-// One atom pair, FP32.  mode selects the field terms and which LJ parameters;
-// mode 0 (a pad atom, or an atom outside every cut-off) adds nothing to the
-// LJ sum.  Pad atoms are inert (q = sigma^6 = eps = 0), so every slot is
-// evaluated without a bounds test.  The LJ term is branch-free (a zero
-// prefactor switches it off), so two calls in a row interleave; the field
-// terms branch only for the multipole variants.
-template <int TYPE>
-__device__ __forceinline__ void pair(const View &m, int k, uint32_t mode, float hx, float hy,
-                                     float hz, float lx, float ly, float lz, Acc &s) {
-  const float4 a = m.a4[k];
-  float2 lj = m.lj[k];
-  if (TYPE == 1 && (mode & M_LJQ)) {
-    const ClusterF32 &C = m.cl[m.cid[k]];
-    lj = make_float2(C.qsig6, C.qeps);
-  }
-  const float eps = (TYPE == 4 || TYPE == 6 || (mode & (M_LJ | M_LJQ))) ? lj.y : 0.0f;
-  const float dx = (hx - a.x) + lx;
-  const float dy = (hy - a.y) + ly;
-  const float dz = (hz - a.z) + lz;
-  const float r2 = dx * dx + dy * dy + dz * dz;
-  const float ir = rsqrtf(r2);
-  const float ir2 = ir * ir;
-  const float s6 = lj.x * (ir2 * ir2 * ir2);
-  const float f = eps * ir2 * s6 * (2.0f * s6 - 1.0f);
-  s.Fx += f * dx; s.Fy += f * dy; s.Fz += f * dz;
-  if (Traits<TYPE>::kCharge && (Traits<TYPE>::kEsAlways || (mode & M_ES))) {
-    const float q3 = a.w * ir * ir2;
-    const float q5 = q3 * ir2;
-    s.Ex += q3 * dx; s.Ey += q3 * dy; s.Ez += q3 * dz;
-    s.Q3 += q3;
-    const float wx = q5 * dx, wy = q5 * dy;
-    s.Pxx += wx * dx; s.Pxy += wx * dy; s.Pxz += wx * dz;
-    s.Pyy += wy * dy; s.Pyz += wy * dz; s.Pzz += q5 * dz * dz;
-  }
-}
-
-struct WorkM { uint32_t lj, es, far; };
-
-// ---- lanes of one trajectory ------------------------------------------------------
-// A narrow group is G <= 32 lanes of one warp: shuffles reduce (bitwise the
-// same sums in every lane), __syncwarp orders the group's shared-memory state.
-struct NarrowLanes {
-  int G, lane;
-  unsigned gmask;
-  __device__ __forceinline__ void sync() const { __syncwarp(gmask); }
-  // the predicate over the whole warp: every group of the warp takes the same
-  // branch, so the full-warp shuffles inside it stay convergent
-  __device__ __forceinline__ bool any(bool p) const { return __any_sync(0xffffffffu, p); }
-  __device__ __forceinline__ bool all(bool p) const { return __all_sync(0xffffffffu, p); }
-  template <typename T, int K>
-  __device__ __forceinline__ void sum(T (&v)[K]) {
-#pragma unroll
-    for (int k = 0; k < K; k++) v[k] = group_sum(v[k], G);
-  }
-};
-
-// Acceleration at pos (FP64 in, FP64 out) for one group.  Pair counts are
-// taken per cluster in pass 1 (or per evaluation), not per pair.
-template <int TYPE, class L>
-__device__ __forceinline__ void force(const View &m, const DevParams &p, const double pos[3],
-                                      double acc[3], L &ln, uint8_t *modes, WorkM &w) {
-  const int G = ln.G, lane = ln.lane;
-  Acc s = {};
-  const float hx = (float)pos[0], hy = (float)pos[1], hz = (float)pos[2];
-  const float lx = (float)(pos[0] - (double)hx), ly = (float)(pos[1] - (double)hy),
-              lz = (float)(pos[2] - (double)hz);
-  if (Traits<TYPE>::kClusters) {
-    // pass 1: near/far decision per cluster (FP64), far-field terms
-    for (int c = lane; c < m.nc; c += G) {
-      const ClusterF32 &C = m.cl[c];
-      const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
-      const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
-      const bool in_disp = !(r2 > C.dr2);
-      uint32_t mode;
-      if (TYPE == 5) {
-        mode = in_disp ? M_LJ : 0;
-      } else if (TYPE == 3) {
-        mode = M_ES | (in_disp ? M_LJ : 0);
-      } else {
-        if (r2 > C.mpr2) {
-          far_terms(m, c, p.multipole_order, (float)d0, (float)d1, (float)d2, s);
-          w.far++;
-          mode = TYPE == 2 ? M_LJ : (in_disp ? M_LJQ : 0);
-        } else {
-          mode = M_ES | ((TYPE == 2 || in_disp) ? M_LJ : 0);
-        }
-      }
-      modes[c] = (uint8_t)mode;
-      if (Traits<TYPE>::kVaryingPairs) {
-        const uint32_t cnt = (uint32_t)(C.a1 - C.a0);
-        if (mode & M_ES) w.es += cnt;
-        else if (mode) w.lj += cnt;
-      }
-    }
-    ln.sync();
-    // pass 2: atom slots, 2G at a time (two independent pairs per lane; G <= 32
-    // and slots come in multiples of 64, so both are in range)
-    for (int base = 0; base < m.nslots; base += 2 * G) {
-      const int k0 = base + lane, k1 = k0 + G;
-      const uint32_t m0 = modes[m.cid[k0]];
-      const uint32_t m1 = modes[m.cid[k1]];
-      pair<TYPE>(m, k0, m0, hx, hy, hz, lx, ly, lz, s);
-      pair<TYPE>(m, k1, m1, hx, hy, hz, lx, ly, lz, s);
-    }
-    ln.sync();
-  } else {
-    constexpr uint32_t mode = TYPE == 4 ? (M_ES | M_LJ) : M_LJ;
-    for (int base = 0; base < m.nslots; base += 2 * G) {
-      const int k0 = base + lane, k1 = k0 + G;
-      pair<TYPE>(m, k0, mode, hx, hy, hz, lx, ly, lz, s);
-      pair<TYPE>(m, k1, mode, hx, hy, hz, lx, ly, lz, s);
-    }
-  }
-  // group reduction (identical result in every lane of the group)
-  constexpr int K = Traits<TYPE>::kFar ? 22 : (Traits<TYPE>::kCharge ? 13 : 3);
-  float v[K];
-  v[0] = s.Fx; v[1] = s.Fy; v[2] = s.Fz;
-  if (Traits<TYPE>::kCharge) {
-    v[3] = s.Ex; v[4] = s.Ey; v[5] = s.Ez;
-    v[6] = s.Pxx; v[7] = s.Pxy; v[8] = s.Pxz; v[9] = s.Pyy; v[10] = s.Pyz; v[11] = s.Pzz;
-    v[12] = s.Q3;
-  }
-  if (Traits<TYPE>::kFar) {
-    v[13] = s.Mdx; v[14] = s.Mdy; v[15] = s.Mdz; v[16] = s.Msxy; v[17] = s.Msxz;
-    v[18] = s.Msyz; v[19] = s.Maxy; v[20] = s.Maxz; v[21] = s.Mayz;
-  }
-  ln.sum(v);
-  acc[0] = v[0]; acc[1] = v[1]; acc[2] = v[2];
-  if (Traits<TYPE>::kCharge) {
-    double Mxx = (double)v[12] - 3.0 * v[6], Myy = (double)v[12] - 3.0 * v[9],
-           Mzz = (double)v[12] - 3.0 * v[11];
-    double Sxy = -3.0 * v[7], Sxz = -3.0 * v[8], Syz = -3.0 * v[10];
-    double Axy = 0, Axz = 0, Ayz = 0;
-    if (Traits<TYPE>::kFar) {
-      Mxx += v[13]; Myy += v[14]; Mzz += v[15];
-      Sxy += v[16]; Sxz += v[17]; Syz += v[18];
-      Axy = v[19]; Axz = v[20]; Ayz = v[21];
-    }
-    const double Ex = v[3], Ey = v[4], Ez = v[5], ds = p.dipole_scalar;
-    acc[0] += ds * (Mxx * Ex + (Sxy + Axy) * Ey + (Sxz + Axz) * Ez);
-    acc[1] += ds * ((Sxy - Axy) * Ex + Myy * Ey + (Syz + Ayz) * Ez);
-    acc[2] += ds * ((Sxz - Axz) * Ex + (Syz - Ayz) * Ey + Mzz * Ez);
-  }
-}
-
-// Exact potential in FP64 (forceAccel.cpp:943-982), lanes split the atoms.
-template <class L>
-__device__ double potential(const View64 &m, const DevParams &p, const double pos[3], L &ln) {
-  double v[4] = {0, 0, 0, 0};
-  for (int k = ln.lane; k < m.n; k += ln.G) {
-    const double *A = reinterpret_cast<const double *>(m.at + k);
-    const double dx = pos[0] - __ldg(A + 0), dy = pos[1] - __ldg(A + 1),
-                 dz = pos[2] - __ldg(A + 2);
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    const double r6 = r2 * r2 * r2;
-    const double term2 = __ldg(A + 4) / r6;
-    v[0] += __ldg(A + 6) * (term2 * term2 - term2);
-    if (p.charged) {
-      const double r_3 = __ldg(A + 3) / (r2 * sqrt(r2));
-      v[1] += dx * r_3; v[2] += dy * r_3; v[3] += dz * r_3;
-    }
-  }
-  ln.sum(v);
-  double total = v[0];
-  if (p.charged) total -= p.dipole_scalar * 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]);
-  return total;
-}
-
-__device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
-  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
-}
-
-__device__ __forceinline__ double angle3(const double a[3], const double b[3]) {
-  double term1 = dot3(a, b);
-  double term2 = sqrt(dot3(a, a)) * sqrt(dot3(b, b));
-  double term3 = term1 / term2;
-  if (term3 > 1) return 0;
-  if (term3 < -1) return COSIMS_PI;
-  return acos(term3);
-}
-
-enum Phase : int { P_ACQUIRE = 0, P_INIT_FIRST, P_INIT_RETRY, P_STEP, P_DONE };
-
-// Trajectory state of one group, in shared memory rather than registers, so
-// the pair loop runs at 64 registers a thread.  Every lane of the group
-// computes the same values (the group sums are bitwise identical in every
-// lane); each update reads the fields it needs, synchronises the group, then
-// writes, so no lane overwrites a value another lane has yet to read.  The
-// group's evaluation counters are kept by its leader lane only.
-struct GroupState {
-  TrajState s;
-  unsigned long long nsteps;
-  uint32_t nforce, npot;
-  unsigned long long lj, es, far;     // pair terms (shared-memory atomics of all lanes)
-};
-static_assert(sizeof(GroupState) == kGroupStateBytes, "GroupState layout");
-
-// Pair counters of one lane (force variants 1, 2, 5), added to the group's
-// counters once the lane is done.
-struct Tally {
-  uint32_t lj = 0, es = 0, far = 0;
-};
-
-__device__ __forceinline__ void group_counters_clear(GroupState &G) {
-  G.nsteps = 0; G.nforce = 0; G.npot = 0; G.lj = 0; G.es = 0; G.far = 0;
-}
-
-// Fold a lane's pair tally into its group (shared-memory atomics, once).
-template <int TYPE>
-__device__ __forceinline__ void fold_tally(GroupState &G, const Tally &tl) {
-  if (Traits<TYPE>::kVaryingPairs) {
-    if (tl.lj) atomicAdd(&G.lj, (unsigned long long)tl.lj);
-    if (tl.es) atomicAdd(&G.es, (unsigned long long)tl.es);
-    if (tl.far) atomicAdd(&G.far, (unsigned long long)tl.far);
-  }
-}
-
-// Group counters, once per group (leader lane) at the end of its work.  For
-// the variants with a fixed pair count the pair terms are n_atoms per
-// acceleration evaluation.
-template <int TYPE>
-__device__ __forceinline__ void flush_group(GroupState &G, int n_atoms, unsigned long long *c) {
-  if (!Traits<TYPE>::kVaryingPairs) {
-    if (Traits<TYPE>::kCharge) G.es = (unsigned long long)G.nforce * n_atoms;
-    else G.lj = (unsigned long long)G.nforce * n_atoms;
-  }
-  const int n_atoms_pot = n_atoms;
-  count_add(c, C_STEPS, (long long)G.nsteps);
-  count_add(c, C_FORCE_EVALS, G.nforce);
-  count_add(c, C_POT_EVALS, G.npot);
-  count_add(c, C_PAIR_POT, (long long)G.npot * n_atoms_pot);
-  count_add(c, C_PAIR_LJ, (long long)G.lj);
-  count_add(c, C_PAIR_ES, (long long)G.es);
-  count_add(c, C_FAR, (long long)G.far);
-  group_counters_clear(G);
-}
-
-// Start a trajectory: slot t, start state p0/v0 (every lane writes the same).
-__device__ __forceinline__ void traj_begin(TrajState &S, long long t, const double *p0,
-                                           const double *v0, double dt, bool may_handoff) {
-  S.t = t;
-  for (int i = 0; i < 3; i++) { S.p0[i] = p0[i]; S.v0[i] = v0[i]; }
-  S.tries = 0; S.max_tries = 8; S.dt = dt; S.step = 0; S.total = 0;
-  S.etries = 0; S.otries = 0;
-  S.may_handoff = may_handoff ? 1 : 0;
-  S.phase = P_INIT_FIRST;
-}
-
-constexpr uint32_t kHandoffSpinLimit = 1u << 22;
-
-// Where a group's trajectories come from.  Narrow groups draw queue slots
-// 0..n-1 (slot k integrates trajectory order[k]; a trajectory with hit[t] == 0
-// is an ellipsoid miss, chi = 0) and may park long ones; wide groups finish
-// parked trajectories.
-struct MainSource {
-  const double *pos0, *vel0;
-  const int32_t *hit, *order;
-  long long n;
-  cosims_traj_out *out;
-  unsigned long long *queue, *counters;
-  Handoff ho;
-};
-
-// The single-molecule kernel reads the same fields straight from its
-// (grid-constant) parameters, so they take no registers.
-struct ArgsSource {
-  const TrajArgs &a;
-};
-
-__device__ __forceinline__ cosims_traj_out *out_of(const MainSource &s) { return s.out; }
-__device__ __forceinline__ cosims_traj_out *out_of(const ArgsSource &s) { return s.a.out; }
-__device__ __forceinline__ long long budget_of(const MainSource &s) { return s.ho.budget; }
-__device__ __forceinline__ long long budget_of(const ArgsSource &s) { return s.a.ho.budget; }
-
-// Acquire the next trajectory into S; false when the source is exhausted.
-template <class A>
-__device__ __forceinline__ bool acquire_main(const A &src, const DevParams &p, NarrowLanes &ln,
-                                             GroupState &GS) {
-  for (;;) {
-    long long tk = 0;
-    if (ln.lane == 0) tk = (long long)atomicAdd(src.queue, 1ull);
-    long long t = __shfl_sync(ln.gmask, tk, 0, ln.G);
-    if (t >= src.n) {
-      // the one group that drew slot n saw the queue empty first
-      if (ln.lane == 0 && src.counters && t == src.n) mark_first(src.counters, C_T_DRAIN_INV);
-      return false;
-    }
-    if (src.order) t = src.order[t];
-    if (src.hit && !src.hit[t]) {               // ellipsoid miss: chi = 0
-      if (ln.lane == 0) {
-        cosims_traj_out o = {0.0, 0.0, 0, 0u};
-        src.out[t] = o;
-      }
-      continue;
-    }
-    traj_begin(GS.s, t, src.pos0 + 3 * t, src.vel0 + 3 * t, p.dt, src.ho.budget > 0);
-    return true;
-  }
-}
-__device__ __forceinline__ bool acquire(const MainSource &src, const DevParams &p,
-                                        NarrowLanes &ln, GroupState &GS) {
-  return acquire_main(src, p, ln, GS);
-}
-__device__ __forceinline__ bool acquire(const ArgsSource &src, const DevParams &p,
-                                        NarrowLanes &ln, GroupState &GS) {
-  return acquire_main(src.a, p, ln, GS);
-}
-
-// Park the trajectory in S for a wide group; false when the record array is
-// full (the group then keeps it).
-__device__ __forceinline__ bool park_to(const Handoff &ho, NarrowLanes &ln, GroupState &GS) {
-  long long r = 0;
-  if (ln.lane == 0) r = (long long)atomicAdd(ho.reserve, 1ull);
-  r = __shfl_sync(ln.gmask, r, 0, ln.G);
-  if (r >= ho.cap) return false;
-  const double *s = reinterpret_cast<const double *>(&GS.s);
-  double *g = reinterpret_cast<double *>(ho.states + r);
-  for (int k = ln.lane; k < kTrajStateBytes / 8; k += ln.G) g[k] = s[k];
-  __threadfence();
-  ln.sync();
-  if (ln.lane == 0) atomicExch(ho.ready + r, 1u);
-  return true;
-}
-__device__ __forceinline__ bool park(const MainSource &src, NarrowLanes &ln, GroupState &GS) {
-  return park_to(src.ho, ln, GS);
-}
-__device__ __forceinline__ bool park(const ArgsSource &src, NarrowLanes &ln, GroupState &GS) {
-  return park_to(src.a.ho, ln, GS);
-}
-
-// The trajectory loop of one group.  Every iteration evaluates one
-// acceleration per group (at the start state or after a position update)
-// and, when any group of the warp needs it, one potential; a group whose
-// trajectory ends takes the next one at once.  The control flow is
-// diffEqSolver::verletVel's (diffEqSolver.cpp:81-211).
-template <int TYPE, class L, class Src>
-__device__ __forceinline__ void group_loop(const View &m, const View64 &m64, const DevParams &p,
-                                           L &ln, uint8_t *modes, GroupState &GS,
-                                           const Src &src, Tally &tl) {
-  TrajState &S = GS.s;
-  const long long cap = p.max_steps > 0 ? p.max_steps : kDefaultMaxSteps;
-
-  while (true) {
-    int phase = S.phase;
-    if (phase == P_ACQUIRE) {
-      ln.sync();
-      const bool got = acquire(src, p, ln, GS);
-      ln.sync();
-      // a new trajectory starts at INIT_FIRST, a parked one where it stopped
-      phase = got ? S.phase : (int)P_DONE;
-      ln.sync();
-      if (!got) S.phase = P_DONE;
-    }
-    if (ln.all(phase == P_DONE)) break;
-
-    double ep[3];
-    bool needU = false, outside = false;
-    if (phase == P_INIT_FIRST || phase == P_INIT_RETRY) {
-      ep[0] = S.p0[0]; ep[1] = S.p0[1]; ep[2] = S.p0[2];
-      needU = phase == P_INIT_FIRST;
-    } else if (phase == P_STEP) {
-      const double dt = S.dt;
-      double vh[3];
-      for (int i = 0; i < 3; i++) {
-        const double a = S.acc[i], v = S.vel[i];
-        ep[i] = S.pos[i] + v * dt + a * dt * dt * 0.5;
-        vh[i] = v + a * dt * 0.5;
-      }
-      const int step = S.step;
-      ln.sync();
-      for (int i = 0; i < 3; i++) { S.pos[i] = ep[i]; S.vel[i] = vh[i]; }
-      const double t0 = ep[0] / p.ell_a, t1 = ep[1] / p.ell_b, t2 = ep[2] / p.ell_c;
-      const double mag2 = t0 * t0 + t1 * t1 + t2 * t2;
-      outside = (mag2 > 1 && p.projection) || (mag2 > p.max_rad && !p.projection);
-      needU = outside && step + 1 > 10;
-    } else {
-      ep[0] = 1.0e4; ep[1] = 0.0; ep[2] = 0.0;
-    }
-    ln.sync();
-
-    double an[3];
-    WorkM wi = {0, 0, 0};
-    force<TYPE>(m, p, ep, an, ln, modes, wi);
-    if (Traits<TYPE>::kVaryingPairs) {
-      tl.lj += wi.lj; tl.es += wi.es; tl.far += wi.far;
-    }
-    double U = 0;
-    if (ln.any(needU)) {
-      double up[3];
-      if (phase == P_STEP) { up[0] = S.pos[0]; up[1] = S.pos[1]; up[2] = S.pos[2]; }
-      else if (phase == P_DONE) { up[0] = 1.0e4; up[1] = 0.0; up[2] = 0.0; }
-      else { up[0] = S.p0[0]; up[1] = S.p0[1]; up[2] = S.p0[2]; }
-      U = potential(m64, p, up, ln);
-    }
-    if (phase == P_DONE) continue;
-    if (ln.lane == 0) {
-      GS.nforce += 1;
-      if (needU) GS.npot += 1;
-    }
-
-    if (phase == P_INIT_FIRST || phase == P_INIT_RETRY) {
-      double p0[3], v0[3];
-      for (int i = 0; i < 3; i++) { p0[i] = S.p0[i]; v0[i] = S.v0[i]; }
-      ln.sync();
-      if (phase == P_INIT_FIRST) S.E0 = U + 0.5 * p.mu * dot3(v0, v0);
-      for (int i = 0; i < 3; i++) { S.acc[i] = an[i]; S.pos[i] = p0[i]; S.vel[i] = v0[i]; }
-      S.orbits = 0;
-      S.rdot = dot3(p0, v0);
-      S.phase = P_STEP;
-      ln.sync();
-      continue;
-    }
-
-    // read the fields this step rewrites, synchronise, then read the rest
-    const double dt = S.dt, rold = S.rdot;
-    double vel[3];
-    for (int i = 0; i < 3; i++) vel[i] = S.vel[i] + an[i] * dt * 0.5;
-    const int step = S.step + 1;
-    const long long total = S.total + 1;
-    int orbits = S.orbits, etries = S.etries, otries = S.otries;
-    double tries = S.tries, max_tries = S.max_tries, dt_new = dt;
-    ln.sync();
-    double pos[3];
-    for (int i = 0; i < 3; i++) pos[i] = S.pos[i];
-    const double E0 = S.E0;
-    const bool may_handoff = S.may_handoff != 0;
-    const long long t = S.t;
-
-    if (ln.lane == 0) GS.nsteps += 1;
-    bool track = true;
-    const double rdot = dot3(pos, vel);
-    if (step > 2 && rdot * rold < 0 && !(rdot > rold)) {
-      orbits++;
-      if (orbits > 8) track = false;
-    }
-    int step_out = step;
-    int next = P_STEP;
-    double chi = COSIMS_PI_2, dE = 0.0;
-    uint32_t status = 0;
-    bool finished = false;
-    if (!track) {
-      tries++;
-      otries++;
-      dt_new = p.dt / (tries + 1);
-    } else if (outside && step > 10) {
-      const double endE = U + 0.5 * p.mu * dot3(vel, vel);
-      dE = 100 * fabs(E0 - endE) / E0;
-      if (dE > 0.5) {
-        tries++;
-        max_tries++;
-        etries++;
-        dt_new = p.dt / (tries + 1);
-        step_out = 0;
-      } else {
-        const double v0[3] = {S.v0[0], S.v0[1], S.v0[2]};
-        chi = angle3(v0, vel);
-        status = COSIMS_TRAJ_HIT | COSIMS_TRAJ_SUCCESS;
-        finished = true;
-      }
-    }
-    if (!finished) {
-      // the step cap, or a state gone non-finite (the reference would loop)
-      if (total >= cap || !isfinite(rdot)) {
-        chi = COSIMS_PI_2; dE = 0.0;
-        status = COSIMS_TRAJ_HIT | COSIMS_TRAJ_STEPCAP;
-        finished = true;
-      } else if (!(tries < max_tries && max_tries < 10)) {
-        chi = COSIMS_PI_2; dE = 0.0;
-        status = COSIMS_TRAJ_HIT;
-        finished = true;
-      } else if (step_out == 0) {
-        next = P_INIT_RETRY;
-      }
-    }
-    if (finished) {
-      if (ln.lane == 0) {
-        cosims_traj_out o;
-        o.chi = chi; o.de_pct = dE; o.steps = step_out;
-        o.status = status | ((uint32_t)etries << COSIMS_TRAJ_ETRIES_SHIFT) |
-                   ((uint32_t)otries << COSIMS_TRAJ_OTRIES_SHIFT);
-        out_of(src)[t] = o;
-      }
-      next = P_ACQUIRE;
-    }
-    for (int i = 0; i < 3; i++) { S.vel[i] = vel[i]; S.acc[i] = an[i]; }
-    S.rdot = rdot; S.orbits = orbits; S.etries = etries; S.otries = otries;
-    S.tries = tries; S.max_tries = max_tries; S.dt = dt_new;
-    S.step = step_out; S.total = total;
-    S.phase = next;
-    ln.sync();
-    // a long trajectory moves to a wide group (deterministic: its own step count)
-    if (!finished && may_handoff && total >= budget_of(src)) {
-      if (park(src, ln, GS)) S.phase = P_ACQUIRE;
-      else S.may_handoff = 0;
-      ln.sync();
-    }
-  }
-}
-
-#ifndef COSIMS_MIXED_MIN_BLOCKS
-#define COSIMS_MIXED_MIN_BLOCKS 1
-#endif
-
-// Dynamic shared memory of the mixed kernels: [F32 image, 16-byte padded]
-// then the groups' scratch.  Narrow phase: [GroupState x groups][cluster modes
-// x groups].  Wide phase (same bytes, after a CTA barrier): per wide group
-// [GroupState][modes][float slots 2 x warps x 24][double slots 2 x warps x 4]
-// [broadcast word].
-__device__ __forceinline__ unsigned char *scratch_base(unsigned char *smem, uint32_t img_bytes) {
-  return smem + ((img_bytes + 15u) & ~15u);
-}
-
-__device__ __forceinline__ void narrow_scratch(unsigned char *smem, uint32_t img_bytes, int G,
-                                               int mode_stride, GroupState *&S,
-                                               uint8_t *&modes) {
-  const int ngroups = blockDim.x / G;
-  const int g = threadIdx.x / G;
-  unsigned char *p = scratch_base(smem, img_bytes);
-  S = reinterpret_cast<GroupState *>(p) + g;
-  modes = p + (size_t)ngroups * sizeof(GroupState) + (size_t)g * mode_stride;
-}
-
-// ---- wide groups: one trajectory per WG threads, latency first ---------------------
-// A parked trajectory is finished by a wide group.  Its state stays in
-// registers (every thread of the group computes the same values: the sums are
-// read from shared memory in warp order by all), each thread evaluates the
-// pair terms of nslots / WG atom slots, and a step costs two barriers: after
-// the cluster pass, and after the per-warp partial sums.  Modes and slots are
-// double-buffered by step parity, so no barrier closes a step.
-struct Wide {
-  int WG, lane, warp, nwarps, bar;
-  uint8_t *modes;     // [2][mode_stride]
-  int mode_stride;
-  float *fslots;      // [2][nwarps][kWideSlotFloats]
-  double *dslots;     // [2][nwarps][4]
-  long long *bcast;
-  __device__ __forceinline__ void sync() const {
-    asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(WG) : "memory");
-  }
-  // sum of v over the group, the same in every thread
-  template <int K>
-  __device__ __forceinline__ void sum(float (&v)[K], int par) const {
-#pragma unroll
-    for (int k = 0; k < K; k++) v[k] = group_sum(v[k], 32);
-    float *slot = fslots + par * nwarps * kWideSlotFloats;
-    if ((lane & 31) == 0) {
-#pragma unroll
-      for (int k = 0; k < K; k++) slot[warp * kWideSlotFloats + k] = v[k];
-    }
-    sync();
-#pragma unroll
-    for (int k = 0; k < K; k++) v[k] = slot[k];
-    for (int w = 1; w < nwarps; w++) {
-#pragma unroll
-      for (int k = 0; k < K; k++) v[k] += slot[w * kWideSlotFloats + k];
-    }
-  }
-  template <int K>
-  __device__ __forceinline__ void sum(double (&v)[K], int par) const {
-#pragma unroll
-    for (int k = 0; k < K; k++) v[k] = group_sum(v[k], 32);
-    double *slot = dslots + par * nwarps * 4;
-    if ((lane & 31) == 0) {
-#pragma unroll
-      for (int k = 0; k < K; k++) slot[warp * 4 + k] = v[k];
-    }
-    sync();
-#pragma unroll
-    for (int k = 0; k < K; k++) v[k] = slot[k];
-    for (int w = 1; w < nwarps; w++) {
-#pragma unroll
-      for (int k = 0; k < K; k++) v[k] += slot[w * 4 + k];
-    }
-  }
-};
-
-template <int TYPE>
-__device__ __forceinline__ void wide_force(const View &m, const DevParams &p, const double pos[3],
-                                           double acc[3], const Wide &wd, int par, Tally &tl) {
-  Acc s = {};
-  const float hx = (float)pos[0], hy = (float)pos[1], hz = (float)pos[2];
-  const float lx = (float)(pos[0] - (double)hx), ly = (float)(pos[1] - (double)hy),
-              lz = (float)(pos[2] - (double)hz);
-  const int lane = wd.lane, WG = wd.WG;
-  if (Traits<TYPE>::kClusters) {
-    uint8_t *modes = wd.modes + par * wd.mode_stride;
-    for (int c = lane; c < m.nc; c += WG) {
-      const ClusterF32 &C = m.cl[c];
-      const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
-      const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
-      const bool in_disp = !(r2 > C.dr2);
-      uint32_t mode;
-      if (TYPE == 5) {
-        mode = in_disp ? M_LJ : 0;
-      } else if (TYPE == 3) {
-        mode = M_ES | (in_disp ? M_LJ : 0);
-      } else {
-        if (r2 > C.mpr2) {
-          far_terms(m, c, p.multipole_order, (float)d0, (float)d1, (float)d2, s);
-          tl.far++;
-          mode = TYPE == 2 ? M_LJ : (in_disp ? M_LJQ : 0);
-        } else {
-          mode = M_ES | ((TYPE == 2 || in_disp) ? M_LJ : 0);
-        }
-      }
-      modes[c] = (uint8_t)mode;
-      if (Traits<TYPE>::kVaryingPairs) {
-        const uint32_t cnt = (uint32_t)(C.a1 - C.a0);
-        if (mode & M_ES) tl.es += cnt;
-        else if (mode) tl.lj += cnt;
-      }
-    }
-    wd.sync();
-    for (int k = lane; k < m.nslots; k += WG) {
-      const uint32_t mk = modes[m.cid[k]];
-      pair<TYPE>(m, k, mk, hx, hy, hz, lx, ly, lz, s);
-    }
-  } else {
-    constexpr uint32_t mode = TYPE == 4 ? (M_ES | M_LJ) : M_LJ;
-    for (int k = lane; k < m.nslots; k += WG) pair<TYPE>(m, k, mode, hx, hy, hz, lx, ly, lz, s);
-  }
-  constexpr int K = Traits<TYPE>::kFar ? 22 : (Traits<TYPE>::kCharge ? 13 : 3);
-  float v[K];
-  v[0] = s.Fx; v[1] = s.Fy; v[2] = s.Fz;
-  if (Traits<TYPE>::kCharge) {
-    v[3] = s.Ex; v[4] = s.Ey; v[5] = s.Ez;
-    v[6] = s.Pxx; v[7] = s.Pxy; v[8] = s.Pxz; v[9] = s.Pyy; v[10] = s.Pyz; v[11] = s.Pzz;
-    v[12] = s.Q3;
-  }
-  if (Traits<TYPE>::kFar) {
-    v[13] = s.Mdx; v[14] = s.Mdy; v[15] = s.Mdz; v[16] = s.Msxy; v[17] = s.Msxz;
-    v[18] = s.Msyz; v[19] = s.Maxy; v[20] = s.Maxz; v[21] = s.Mayz;
-  }
-  wd.sum(v, par);
-  acc[0] = v[0]; acc[1] = v[1]; acc[2] = v[2];
-  if (Traits<TYPE>::kCharge) {
-    double Mxx = (double)v[12] - 3.0 * v[6], Myy = (double)v[12] - 3.0 * v[9],
-           Mzz = (double)v[12] - 3.0 * v[11];
-    double Sxy = -3.0 * v[7], Sxz = -3.0 * v[8], Syz = -3.0 * v[10];
-    double Axy = 0, Axz = 0, Ayz = 0;
-    if (Traits<TYPE>::kFar) {
-      Mxx += v[13]; Myy += v[14]; Mzz += v[15];
-      Sxy += v[16]; Sxz += v[17]; Syz += v[18];
-      Axy = v[19]; Axz = v[20]; Ayz = v[21];
-    }
-    const double Ex = v[3], Ey = v[4], Ez = v[5], ds = p.dipole_scalar;
-    acc[0] += ds * (Mxx * Ex + (Sxy + Axy) * Ey + (Sxz + Axz) * Ez);
-    acc[1] += ds * ((Sxy - Axy) * Ex + Myy * Ey + (Syz + Ayz) * Ez);
-    acc[2] += ds * ((Sxz - Axz) * Ex + (Syz - Ayz) * Ey + Mzz * Ez);
-  }
-}
-
-__device__ __forceinline__ double wide_potential(const View64 &m, const DevParams &p,
-                                                 const double pos[3], const Wide &wd, int par) {
-  double v[4] = {0, 0, 0, 0};
-  for (int k = wd.lane; k < m.n; k += wd.WG) {
-    const double *A = reinterpret_cast<const double *>(m.at + k);
-    const double dx = pos[0] - __ldg(A + 0), dy = pos[1] - __ldg(A + 1),
-                 dz = pos[2] - __ldg(A + 2);
-    const double r2 = dx * dx + dy * dy + dz * dz;
-    const double r6 = r2 * r2 * r2;
-    const double term2 = __ldg(A + 4) / r6;
-    v[0] += __ldg(A + 6) * (term2 * term2 - term2);
-    if (p.charged) {
-      const double r_3 = __ldg(A + 3) / (r2 * sqrt(r2));
-      v[1] += dx * r_3; v[2] += dy * r_3; v[3] += dz * r_3;
-    }
-  }
-  wd.sum(v, par);
-  double total = v[0];
-  if (p.charged) total -= p.dipole_scalar * 0.5 * (v[1] * v[1] + v[2] * v[2] + v[3] * v[3]);
-  return total;
-}
-
-// Take the next parked record; -1 when none is left (the same in every thread).
-__device__ __forceinline__ long long wide_take(const Wide &wd, const Handoff &ho,
-                                               unsigned long long *counters) {
-  if (wd.lane == 0) {
-    long long got = -1;
-    unsigned long long tk = atomicAdd(ho.taken, 0ull);
-    for (uint32_t it = 0; it < 4096u; ++it) {
-      const unsigned long long avail = atomicAdd(ho.reserve, 0ull);
-      const unsigned long long lim = avail < (unsigned long long)ho.cap
-                                         ? avail : (unsigned long long)ho.cap;
-      if (tk >= lim) break;
-      const unsigned long long prev = atomicCAS(ho.taken, tk, tk + 1);
-      if (prev == tk) { got = (long long)tk; break; }
-      tk = prev;
-    }
-    if (got >= 0) {
-      // the parking group reserved the record before writing it: wait for its flag
-      bool ok = false;
-      for (uint32_t spin = 0; spin < kHandoffSpinLimit; ++spin) {
-        if (atomicAdd(ho.ready + got, 0u) != 0u) { ok = true; break; }
-      }
-      if (!ok) {
-        atomicOr(counters + C_ERROR, 2ull);
-        got = -1;
-      }
-      __threadfence();
-    }
-    *wd.bcast = got;
-  }
-  wd.sync();
-  return *wd.bcast;   // rewritten only after the next trajectory's barriers
-}
-
-// The trajectory loop of a wide group over parked records: the control flow
-// of diffEqSolver::verletVel (diffEqSolver.cpp:81-211) from where the narrow
-// group stopped.
-template <int TYPE>
-__device__ __forceinline__ void wide_loop(const View &m, const View64 &m64, const DevParams &p,
-                                          const Wide &wd, const Handoff &ho,
-                                          cosims_traj_out *out, unsigned long long *counters,
-                                          Tally &tl, unsigned long long &nsteps, uint32_t &nforce,
-                                          uint32_t &npot) {
-  const long long cap = p.max_steps > 0 ? p.max_steps : kDefaultMaxSteps;
-  int par = 0;        // step parity: which half of the modes and slots
-  for (;;) {
-    const long long idx = wide_take(wd, ho, counters);
-    if (idx < 0) break;
-    const TrajState *R = ho.states + idx;
-    double pos[3], vel[3], acc[3];
-    for (int i = 0; i < 3; i++) {
-      pos[i] = __ldcg(&R->pos[i]); vel[i] = __ldcg(&R->vel[i]); acc[i] = __ldcg(&R->acc[i]);
-    }
-    double dt = __ldcg(&R->dt), rdot = __ldcg(&R->rdot);
-    int tries = (int)__ldcg(&R->tries), max_tries = (int)__ldcg(&R->max_tries);
-    long long total = __ldcg(&R->total);
-    int step = __ldcg(&R->step), orbits = __ldcg(&R->orbits), phase = __ldcg(&R->phase);
-    int etries = __ldcg(&R->etries), otries = __ldcg(&R->otries);
-    for (;;) {
-      // evaluation point: the start state (retry) or the Verlet position update
-      bool outside = false, needU = false;
-      if (phase == P_INIT_RETRY) {
-        for (int i = 0; i < 3; i++) pos[i] = __ldcg(&R->p0[i]);
-      } else {
-        for (int i = 0; i < 3; i++) {
-          pos[i] = pos[i] + vel[i] * dt + acc[i] * dt * dt * 0.5;
-          vel[i] = vel[i] + acc[i] * dt * 0.5;
-        }
-        const double t0 = pos[0] / p.ell_a, t1 = pos[1] / p.ell_b, t2 = pos[2] / p.ell_c;
-        const double mag2 = t0 * t0 + t1 * t1 + t2 * t2;
-        outside = (mag2 > 1 && p.projection) || (mag2 > p.max_rad && !p.projection);
-        needU = outside && step + 1 > 10;
-      }
-      double an[3];
-      wide_force<TYPE>(m, p, pos, an, wd, par, tl);
-      double U = 0;
-      if (needU) U = wide_potential(m64, p, pos, wd, par);
-      par ^= 1;
-      if (wd.lane == 0) { nforce++; if (needU) npot++; }
-      if (phase == P_INIT_RETRY) {
-        for (int i = 0; i < 3; i++) { vel[i] = __ldcg(&R->v0[i]); acc[i] = an[i]; }
-        orbits = 0;
-        rdot = dot3(pos, vel);
-        phase = P_STEP;
-        continue;
-      }
-      for (int i = 0; i < 3; i++) { vel[i] = vel[i] + an[i] * dt * 0.5; acc[i] = an[i]; }
-      step++;
-      total++;
-      if (wd.lane == 0) nsteps++;
-      bool track = true;
-      const double rold = rdot;
-      rdot = dot3(pos, vel);
-      if (step > 2 && rdot * rold < 0 && !(rdot > rold)) {
-        orbits++;
-        if (orbits > 8) track = false;
-      }
-      bool finished = false;
-      double chi = COSIMS_PI_2, dE = 0.0;
-      uint32_t status = COSIMS_TRAJ_HIT;
-      if (!track) {
-        tries++;
-        otries++;
-        dt = p.dt / ((double)tries + 1);
-      } else if (outside && step > 10) {
-        const double E0 = __ldcg(&R->E0);
-        const double endE = U + 0.5 * p.mu * dot3(vel, vel);
-        dE = 100 * fabs(E0 - endE) / E0;
-        if (dE > 0.5) {
-          tries++;
-          max_tries++;
-          etries++;
-          dt = p.dt / ((double)tries + 1);
-          step = 0;
-          dE = 0.0;
-        } else {
-          double v0[3];
-          for (int i = 0; i < 3; i++) v0[i] = __ldcg(&R->v0[i]);
-          chi = angle3(v0, vel);
-          status |= COSIMS_TRAJ_SUCCESS;
-          finished = true;
-        }
-      }
-      if (!finished) {
-        if (total >= cap || !isfinite(rdot)) {
-          status |= COSIMS_TRAJ_STEPCAP;
-          finished = true;
-        } else if (!(tries < max_tries && max_tries < 10)) {
-          finished = true;
-        } else if (step == 0) {
-          phase = P_INIT_RETRY;
-        }
-      }
-      if (finished) {
-        if (wd.lane == 0) {
-          cosims_traj_out o;
-          o.chi = chi; o.de_pct = dE; o.steps = step;
-          o.status = status | ((uint32_t)etries << COSIMS_TRAJ_ETRIES_SHIFT) |
-                     ((uint32_t)otries << COSIMS_TRAJ_OTRIES_SHIFT);
-          out[__ldcg(&R->t)] = o;
-        }
-        break;
-      }
-    }
-  }
-}
-
-// Wide phase of one CTA: groups of ho.wide_lanes threads finish parked
-// trajectories.  Called by every thread of the CTA after the narrow phase.
-template <int TYPE>
-__device__ __noinline__ void wide_phase(unsigned char *smem, uint32_t img_bytes, const View m,
-                                        const View64 m64, const DevParams &p, int mode_stride,
-                                        const Handoff &ho, cosims_traj_out *out,
-                                        unsigned long long *counters) {
-  const int WG = ho.wide_lanes;
-  const int nwide = blockDim.x / WG;
-  const int wg = threadIdx.x / WG;
-  if (wg >= nwide) return;           // threads beyond whole wide groups sit out
-  unsigned char *base = scratch_base(smem, img_bytes) + (size_t)wg * wide_group_bytes(WG, mode_stride);
-  Wide wd;
-  wd.WG = WG;
-  wd.lane = threadIdx.x - wg * WG;
-  wd.warp = wd.lane >> 5;
-  wd.nwarps = WG >> 5;
-  wd.bar = 1 + wg;
-  wd.modes = base;
-  wd.mode_stride = mode_stride;
-  unsigned char *q = base + ((2u * (uint32_t)mode_stride + 15u) & ~15u);
-  wd.fslots = reinterpret_cast<float *>(q);
-  wd.dslots = reinterpret_cast<double *>(q + 2u * wd.nwarps * kWideSlotFloats * 4u);
-  wd.bcast = reinterpret_cast<long long *>(q + 2u * wd.nwarps * kWideSlotFloats * 4u +
-                                           2u * wd.nwarps * 4u * 8u);
-  if (Traits<TYPE>::kClusters && wd.lane == 0) {
-    wd.modes[m.nc] = 0;                      // the pad atoms' cluster, both halves
-    wd.modes[mode_stride + m.nc] = 0;
-  }
-  wd.sync();
-  Tally tl;
-  unsigned long long nsteps = 0;
-  uint32_t nforce = 0, npot = 0;
-  const unsigned long long t0 = global_ns();
-  wide_loop<TYPE>(m, m64, p, wd, ho, out, counters, tl, nsteps, nforce, npot);
-  if (Traits<TYPE>::kVaryingPairs) {
-    count_add(counters, C_PAIR_LJ, tl.lj);
-    count_add(counters, C_PAIR_ES, tl.es);
-    count_add(counters, C_FAR, tl.far);
-  }
-  if (wd.lane == 0) {
-    count_add(counters, C_WIDE_STEPS, (long long)nsteps);
-    count_add(counters, C_WIDE_NS, (long long)(global_ns() - t0));
-    count_add(counters, C_STEPS, (long long)nsteps);
-    count_add(counters, C_FORCE_EVALS, nforce);
-    count_add(counters, C_POT_EVALS, npot);
-    count_add(counters, C_PAIR_POT, (long long)npot * m64.n);
-    if (!Traits<TYPE>::kVaryingPairs)
-      count_add(counters, Traits<TYPE>::kCharge ? C_PAIR_ES : C_PAIR_LJ,
-                (long long)nforce * m64.n);
-  }
-}
-
-// Threads per CTA at most: 768 gives 80 registers a thread, enough for the
-// wide groups' register-resident state and the far-field sums of variants 1
-// and 2 (the narrow phase runs as fast at 24 warps per SM as at 32).
-template <int TYPE>
-struct KernelShape {
-  static constexpr int kMaxThreads = kMixedMaxBlock;
-};
-
-// SMEM: the F32 image is staged in shared memory (else read from global
-// memory through L1); a separate instantiation, so the pair loop's loads are
-// shared-memory loads with 32-bit addresses.
-template <int TYPE, bool SMEM>
-__global__ void __launch_bounds__(KernelShape<TYPE>::kMaxThreads, COSIMS_MIXED_MIN_BLOCKS)
-    traj_mixed_kernel(const __grid_constant__ TrajArgs a) {
-  extern __shared__ __align__(128) unsigned char smem[];
-  __shared__ uint64_t bar;
-  const unsigned char *base = a.img.gbase;
-  if (SMEM) {
-    if (!stage_to_smem(smem, a.img.gbase, a.img.bytes, &bar, 0, true)) {
-      if (threadIdx.x == 0) atomicOr(a.counters + C_ERROR, 1ull);
-      return;
-    }
-    base = smem;
-  }
-  if (threadIdx.x == 0) mark_first(a.counters, C_T_START_INV);
-  const View m = make_view(base, a.img);
-  const View64 m64 = make_view64(a.img64);
-  const int G = a.group_lanes;
-  const uint32_t img_bytes = SMEM ? a.img.bytes : 0u;
-  GroupState *S;
-  uint8_t *modes;
-  narrow_scratch(smem, img_bytes, G, a.mode_stride, S, modes);
-  NarrowLanes ln;
-  ln.G = G;
-  ln.lane = threadIdx.x & (G - 1);
-  ln.gmask = G == 32 ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
-  if (ln.lane == 0) {
-    S->s.phase = P_ACQUIRE;
-    group_counters_clear(*S);
-    if (Traits<TYPE>::kClusters) modes[m.nc] = 0;    // the pad atoms' cluster
-  }
-  __syncwarp();
-  const ArgsSource src{a};
-  Tally tl;
-  group_loop<TYPE>(m, m64, a.par, ln, modes, *S, src, tl);
-  fold_tally<TYPE>(*S, tl);
-  __syncwarp();
-  if (ln.lane == 0) flush_group<TYPE>(*S, m64.n, a.counters);
-  if (a.ho.budget > 0) {
-    __syncthreads();     // the narrow groups' scratch is reused
-    wide_phase<TYPE>(smem, img_bytes, m, m64, a.par, a.mode_stride, a.ho, a.out, a.counters);
-  }
-  if ((threadIdx.x & 31) == 0) mark_last(a.counters, C_T_END);
-}
 
 // ---- batched form: one persistent launch over many molecules ------------------
 // CTAs take work items (a molecule and a range of its trajectories) from a
@@ -1155,42 +106,20 @@ __global__ void __launch_bounds__(kBatchMaxBlock, 1) batch_mixed_kernel(const Ba
   if (threadIdx.x == 0) mark_last(a.counters, C_T_END);
 }
 
-template <int TYPE, bool SMEM>
-int launch_t(const TrajArgs &a, int block, int grid, size_t smem, void *stream) {
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(traj_mixed_kernel<TYPE, SMEM>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return (int)e;
-  }
-  traj_mixed_kernel<TYPE, SMEM><<<grid, block, smem, (cudaStream_t)stream>>>(a);
-  return (int)cudaGetLastError();
-}
-
-template <int TYPE>
-int launch_s(const TrajArgs &a, int block, int grid, size_t smem, void *stream) {
-  return a.use_smem ? launch_t<TYPE, true>(a, block, grid, smem, stream)
-                    : launch_t<TYPE, false>(a, block, grid, smem, stream);
-}
-
-template <int TYPE, bool SMEM>
-int occupancy_t(int block, size_t smem, int *per_sm) {
-  if (block > KernelShape<TYPE>::kMaxThreads) { *per_sm = 0; return 0; }
-  if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(traj_mixed_kernel<TYPE, SMEM>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return (int)e;
-  }
-  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, traj_mixed_kernel<TYPE, SMEM>,
-                                                            block, smem);
-}
-
-template <int TYPE>
-int occupancy_s(int use_smem, int block, size_t smem, int *per_sm) {
-  return use_smem ? occupancy_t<TYPE, true>(block, smem, per_sm)
-                  : occupancy_t<TYPE, false>(block, smem, per_sm);
-}
-
 }  // namespace mixed
+
+int mixed_launch_t1(const TrajArgs &, int, int, size_t, void *);
+int mixed_launch_t2(const TrajArgs &, int, int, size_t, void *);
+int mixed_launch_t3(const TrajArgs &, int, int, size_t, void *);
+int mixed_launch_t4(const TrajArgs &, int, int, size_t, void *);
+int mixed_launch_t5(const TrajArgs &, int, int, size_t, void *);
+int mixed_launch_t6(const TrajArgs &, int, int, size_t, void *);
+int mixed_occupancy_t1(int, int, int, size_t, int *);
+int mixed_occupancy_t2(int, int, int, size_t, int *);
+int mixed_occupancy_t3(int, int, int, size_t, int *);
+int mixed_occupancy_t4(int, int, int, size_t, int *);
+int mixed_occupancy_t5(int, int, int, size_t, int *);
+int mixed_occupancy_t6(int, int, int, size_t, int *);
 
 int batch_launch(const BatchArgs &a, int block, int grid, size_t smem, void *stream) {
   if (smem > 48 * 1024) {
@@ -1214,23 +143,24 @@ int batch_occupancy(int block, size_t smem, int *per_sm) {
 
 int mixed_launch(const TrajArgs &a, int block, int grid, size_t smem, void *stream) {
   switch (a.par.force_type) {
-    case 1: return mixed::launch_s<1>(a, block, grid, smem, stream);
-    case 2: return mixed::launch_s<2>(a, block, grid, smem, stream);
-    case 3: return mixed::launch_s<3>(a, block, grid, smem, stream);
-    case 4: return mixed::launch_s<4>(a, block, grid, smem, stream);
-    case 5: return mixed::launch_s<5>(a, block, grid, smem, stream);
-    default: return mixed::launch_s<6>(a, block, grid, smem, stream);
+    case 1: return mixed_launch_t1(a, block, grid, smem, stream);
+    case 2: return mixed_launch_t2(a, block, grid, smem, stream);
+    case 3: return mixed_launch_t3(a, block, grid, smem, stream);
+    case 4: return mixed_launch_t4(a, block, grid, smem, stream);
+    case 5: return mixed_launch_t5(a, block, grid, smem, stream);
+    default: return mixed_launch_t6(a, block, grid, smem, stream);
   }
 }
 
-int mixed_occupancy(int force_type, int use_smem, int block, size_t smem, int *per_sm) {
+int mixed_occupancy(int force_type, int use_smem, int group_lanes, int block, size_t smem,
+                    int *per_sm) {
   switch (force_type) {
-    case 1: return mixed::occupancy_s<1>(use_smem, block, smem, per_sm);
-    case 2: return mixed::occupancy_s<2>(use_smem, block, smem, per_sm);
-    case 3: return mixed::occupancy_s<3>(use_smem, block, smem, per_sm);
-    case 4: return mixed::occupancy_s<4>(use_smem, block, smem, per_sm);
-    case 5: return mixed::occupancy_s<5>(use_smem, block, smem, per_sm);
-    default: return mixed::occupancy_s<6>(use_smem, block, smem, per_sm);
+    case 1: return mixed_occupancy_t1(use_smem, group_lanes, block, smem, per_sm);
+    case 2: return mixed_occupancy_t2(use_smem, group_lanes, block, smem, per_sm);
+    case 3: return mixed_occupancy_t3(use_smem, group_lanes, block, smem, per_sm);
+    case 4: return mixed_occupancy_t4(use_smem, group_lanes, block, smem, per_sm);
+    case 5: return mixed_occupancy_t5(use_smem, group_lanes, block, smem, per_sm);
+    default: return mixed_occupancy_t6(use_smem, group_lanes, block, smem, per_sm);
   }
 }
 
