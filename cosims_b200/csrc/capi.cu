@@ -99,6 +99,7 @@ DevParams make_dev_params(const cosims_params *p) {
   d.dt = p->dt; d.mu = p->mu; d.dipole_scalar = p->dipole_scalar;
   d.r_disp = p->r_disp; d.r_mp = p->r_mp;
   d.ell_a = p->ell_a; d.ell_b = p->ell_b; d.ell_c = p->ell_c;
+  d.inv_ell_a = 1.0 / p->ell_a; d.inv_ell_b = 1.0 / p->ell_b; d.inv_ell_c = 1.0 / p->ell_c;
   d.max_rad = std::max(p->ell_a, std::max(p->ell_b, p->ell_c));   // diffEqSolver.cpp:99
   d.b_max = p->b_max; d.start_dist = p->start_dist;
   d.g_min = p->g_min; d.g_max = p->g_max;

@@ -88,6 +88,7 @@ struct DevParams {
   int32_t charged;
   double dt, mu, dipole_scalar, r_disp, r_mp;
   double ell_a, ell_b, ell_c, max_rad;
+  double inv_ell_a, inv_ell_b, inv_ell_c;   // mixed form: 1 / axis (exit test by products)
   double b_max, start_dist, g_min, g_max, vdist_a, vdist_norm, vdist_max;
   double ccs_const;
   int64_t max_steps;
@@ -151,7 +152,7 @@ __host__ __device__ inline uint32_t wide_group_bytes(int wide_lanes, int mode_st
   b += 16u;
   return b;
 }
-constexpr int64_t kDefaultHandoffBudget = 1024;   // steps before a trajectory goes wide
+constexpr int64_t kDefaultHandoffBudget = 2048;   // steps before a trajectory goes wide
 inline int default_wide_lanes(int n_atoms) { return n_atoms <= 1024 ? 128 : 256; }
 
 struct TrajArgs {

@@ -540,7 +540,8 @@ __device__ __forceinline__ void group_loop(const View &m, const View64 &m64, con
       const int step = S.step;
       ln.sync();
       for (int i = 0; i < 3; i++) { S.pos[i] = ep[i]; S.vel[i] = vh[i]; }
-      const double t0 = ep[0] / p.ell_a, t1 = ep[1] / p.ell_b, t2 = ep[2] / p.ell_c;
+      // the ellipsoid exit test by reciprocal axes (no FP64 division per step)
+      const double t0 = ep[0] * p.inv_ell_a, t1 = ep[1] * p.inv_ell_b, t2 = ep[2] * p.inv_ell_c;
       const double mag2 = t0 * t0 + t1 * t1 + t2 * t2;
       outside = (mag2 > 1 && p.projection) || (mag2 > p.max_rad && !p.projection);
       needU = outside && step + 1 > 10;
@@ -782,12 +783,14 @@ __device__ __forceinline__ void wide_force(const View &m, const DevParams &p, co
       }
     }
     wd.sync();
+#pragma unroll 4
     for (int k = lane; k < m.nslots; k += WG) {
       const float4 a = m.a4[k], b = m.b4[k];
       pair<TYPE>(m, a, b, (uint32_t)modes[cluster_of(b)], hx, hy, hz, lx, ly, lz, s);
     }
   } else {
     constexpr uint32_t mode = TYPE == 4 ? (M_ES | M_LJ) : M_LJ;
+#pragma unroll 4
     for (int k = lane; k < m.nslots; k += WG) {
       const float4 a = m.a4[k], b = m.b4[k];
       pair<TYPE>(m, a, b, mode, hx, hy, hz, lx, ly, lz, s);
@@ -913,7 +916,8 @@ __device__ __forceinline__ void wide_loop(const View &m, const View64 &m64, cons
           pos[i] = pos[i] + vel[i] * dt + acc[i] * dt * dt * 0.5;
           vel[i] = vel[i] + acc[i] * dt * 0.5;
         }
-        const double t0 = pos[0] / p.ell_a, t1 = pos[1] / p.ell_b, t2 = pos[2] / p.ell_c;
+        const double t0 = pos[0] * p.inv_ell_a, t1 = pos[1] * p.inv_ell_b,
+                     t2 = pos[2] * p.inv_ell_c;
         const double mag2 = t0 * t0 + t1 * t1 + t2 * t2;
         outside = (mag2 > 1 && p.projection) || (mag2 > p.max_rad && !p.projection);
         needU = outside && step + 1 > 10;

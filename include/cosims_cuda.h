@@ -190,7 +190,7 @@ cosims_status cosims_ctx_get_launch(const cosims_ctx *ctx, int32_t *group_lanes,
  * by a wide group of wide_lanes threads once SMs run out of other work, so
  * the few very long trajectories no longer set the run time.  Results depend
  * only on the trajectory, group_lanes, step_budget and wide_lanes, not on
- * timing.  step_budget: 0 = default (1024), < 0 = off; wide_lanes: 0 =
+ * timing.  step_budget: 0 = default (2048), < 0 = off; wide_lanes: 0 =
  * default (128 up to 1024 atoms, else 256), else a multiple of 32 up to 512.
  * The context keeps a 200-byte record per trajectory of a call for this; calls
  * of more than 2^22 trajectories run without hand-off. */

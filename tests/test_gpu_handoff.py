@@ -61,7 +61,7 @@ def test_handoff_settings_validated():
         with pytest.raises(engine.CosimsError):
             cm.set_handoff(0, 48)                # not a multiple of 32
         cm.set_handoff(0, 0)
-        assert cm.get_handoff()[0] == 1024       # default budget
+        assert cm.get_handoff()[0] == 2048       # default budget
     with engine.Context(mol, par, abi.PLAIN_F64) as cp:
         with pytest.raises(engine.CosimsError):
             cp.set_handoff(100, 128)             # the plain form has no hand-off
