@@ -7,9 +7,14 @@
 // round_traj trajectories of every active job in one launch of the persistent
 // multi-molecule kernel, adds each job's chunk sums to its running sums (on
 // the device, in round order) and retires the jobs whose relative standard
-// error reached the target.  A job's k-th chunk is always trajectories
-// [k*round_traj, (k+1)*round_traj) of its own Philox stream, so its result is
-// the same whether it ran alone or among other jobs.
+// error reached the target.  A job's first chunk is round_traj trajectories;
+// each later chunk is the job's own estimate of what it still needs, from its
+// running error (at most 16 round_traj), so a job typically retires in two or
+// three rounds.  The chunks are always the next trajectories of the job's own
+// Philox stream and their sizes follow from the job alone, so its result is
+// the same whether it ran alone or among other jobs; a round takes jobs in
+// submission order while their chunks fit the server's trajectory slots, and
+// a job that does not fit waits for the next round.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <chrono>
@@ -26,6 +31,7 @@ namespace {
 
 constexpr int kServeBlock = kBatchMaxBlock;
 constexpr uint32_t kServeImageCap = 96 * 1024;
+constexpr int64_t kMaxChunkRounds = 16;   // a chunk is at most 16 round_traj
 
 struct Job {
   int64_t id = 0;
@@ -35,6 +41,7 @@ struct Job {
   int32_t n_atoms = 0;
   double target = 0;
   int64_t min_traj = 0, max_traj = 0, done = 0;
+  int64_t next_chunk = 0;          // trajectories of the job's next round
   int64_t footprint = 0;
   unsigned char *d_img = nullptr;
   BatchMol bm{};
@@ -166,6 +173,7 @@ cosims_status cosims_serve_submit(cosims_server *s, const cosims_molecule *mol,
   j.max_traj = max_traj;
   j.n_atoms = mol->n_atoms;
   j.footprint = fp;
+  j.next_chunk = std::max<int64_t>(s->round_traj, std::min<int64_t>(min_traj, kMaxChunkRounds * s->round_traj));
   const size_t o32 = (h64.img.bytes + 255) & ~size_t(255);
   cudaError_t e = cudaMalloc((void **)&j.d_img, o32 + h32.img.bytes);
   if (e == cudaSuccess) e = cudaMemcpy(j.d_img, h64.bytes.data(), h64.img.bytes, cudaMemcpyHostToDevice);
@@ -198,9 +206,20 @@ cosims_status cosims_serve_step(cosims_server *s, void *stream, int32_t *n_finis
   if (n_finished) *n_finished = 0;
   DeviceGuard g(s->device);
   cudaStream_t st = (cudaStream_t)stream;
+  // jobs in submission order while their chunks fit the trajectory slots
+  const int64_t pool = (int64_t)s->max_jobs * s->round_traj;
   std::vector<Job *> act;
-  for (auto &kv : s->jobs)
-    if (kv.second.state == COSIMS_JOB_RUNNING) act.push_back(&kv.second);
+  std::vector<int64_t> chunk;
+  int64_t packed = 0;
+  for (auto &kv : s->jobs) {
+    Job &j = kv.second;
+    if (j.state != COSIMS_JOB_RUNNING) continue;
+    const int64_t c = std::min<int64_t>(j.next_chunk, j.max_traj - j.done);
+    if (packed + c > pool) continue;
+    act.push_back(&j);
+    chunk.push_back(c);
+    packed += c;
+  }
   if (act.empty()) return COSIMS_OK;
   std::vector<BatchMol> mols;
   std::vector<int32_t> slots;
@@ -212,7 +231,7 @@ cosims_status cosims_serve_step(cosims_server *s, void *stream, int32_t *n_finis
     Job &j = *act[k];
     BatchMol bm = j.bm;
     bm.base = base;
-    bm.n_traj = std::min<int64_t>(s->round_traj, j.max_traj - j.done);
+    bm.n_traj = chunk[k];
     bm.first_index = j.done;
     const size_t need = batch_mol_smem(bm, kServeBlock, budget, kServeImageCap);
     if ((int)need > budget)
@@ -290,10 +309,23 @@ cosims_status cosims_serve_step(cosims_server *s, void *stream, int32_t *n_finis
     j.sums = s->running_host[j.slot];
     const double ne = (double)j.sums.n_eff;
     bool done = j.done >= j.max_traj;
-    if (!done && j.done >= j.min_traj && ne > 1 && j.sums.sum > 0) {
+    double rel = 0;
+    if (!done && ne > 1 && j.sums.sum > 0) {
       const double m = j.sums.sum / ne;
       const double se = std::sqrt(std::max(j.sums.sum2 / ne - m * m, 0.0) / ne);
-      done = se / m <= j.target;
+      rel = se / m;
+      done = j.done >= j.min_traj && rel <= j.target;
+    }
+    if (!done) {
+      // the error falls as 1/sqrt(n): trajectories still needed, plus 5 %
+      int64_t want = s->round_traj;
+      if (rel > 0) {
+        const double need = (double)j.done * ((rel / j.target) * (rel / j.target) - 1.0) * 1.05;
+        want = (int64_t)std::ceil(std::max(need, 0.0) / (double)s->round_traj) * s->round_traj;
+      }
+      want = std::max<int64_t>(want, j.min_traj - j.done);
+      const int64_t cap = std::min<int64_t>(kMaxChunkRounds * s->round_traj, pool);
+      j.next_chunk = std::min<int64_t>(std::max<int64_t>(want, s->round_traj), cap);
     }
     if (done) {
       j.state = COSIMS_JOB_DONE;

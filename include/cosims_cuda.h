@@ -315,11 +315,15 @@ cosims_status cosims_batch_counters(cosims_batch *b, cosims_ccs_sums *work, floa
 /* No counterpart in the reference (it computes one molecule per process).
  * Jobs are admitted while their device footprint fits the HBM budget and a
  * slot is free; each job's molecule and running sums stay on the device.  A
- * round integrates the next round_traj trajectories of every running job in
- * one persistent launch and retires jobs whose relative standard error
- * reached their target (or that reached max_traj).  A job's k-th round is
- * always trajectories [k*round_traj, (k+1)*round_traj) of its own stream, so
- * its result does not depend on the other jobs. */
+ * round integrates the next chunk of every running job that fits the
+ * server's max_jobs * round_traj trajectory slots (submission order) in one
+ * persistent launch, and retires jobs whose relative standard error reached
+ * their target (or that reached max_traj).  A job's first chunk is round_traj
+ * trajectories (or min_traj); later chunks are what its running error says it
+ * still needs (+5 %, in multiples of round_traj, at most 16 round_traj).
+ * Chunks are the next trajectories of the job's own stream and their sizes
+ * follow from the job alone, so its result does not depend on the other
+ * jobs. */
 typedef struct cosims_server cosims_server;
 
 #define COSIMS_JOB_RUNNING 1
