@@ -22,7 +22,8 @@ namespace {
 
 constexpr uint32_t kBatchImageCap = 96 * 1024;   // larger F32 images are read through L1/L2
 constexpr int kBatchBlock = kBatchMaxBlock;
-constexpr int kTrajPerGroupPerItem = 16;
+constexpr int kItemsPerCta = 3;          // items of about equal cost per CTA of a run
+constexpr int kMinTrajPerGroup = 4;      // an item gives every group some trajectories
 
 // process-wide tuning cache: (force type, atom-count class) -> lanes per trajectory
 std::mutex g_tune_mu;
@@ -51,6 +52,41 @@ size_t batch_mol_smem(BatchMol &bm, int block, int budget, uint32_t img_cap) {
     need = scratch;
   }
   return need;
+}
+
+// Work items for one persistent launch: molecule i's n_traj[i] trajectories
+// cut into items of about equal cost (atoms x trajectories), about
+// kItemsPerCta per CTA, so a CTA works on few molecules and rarely waits for
+// its groups to restage; every group of a CTA gets at least kMinTrajPerGroup
+// trajectories of an item.  Largest first, a molecule's items adjacent.
+void balanced_items(const std::vector<int64_t> &n_traj, const std::vector<int> &n_atoms,
+                    const std::vector<int> &group_lanes, int block, int grid,
+                    std::vector<BatchItem> &items) {
+  items.clear();
+  double total = 0;
+  for (size_t m = 0; m < n_traj.size(); m++) total += (double)n_atoms[m] * (double)n_traj[m];
+  const double target = total / (double)std::max(1, kItemsPerCta * std::max(grid, 1));
+  for (size_t m = 0; m < n_traj.size(); m++) {
+    if (n_traj[m] <= 0) continue;
+    const double cost = (double)n_atoms[m] * (double)n_traj[m];
+    int64_t k = std::max<int64_t>(1, (int64_t)std::ceil(cost / std::max(target, 1.0)));
+    const int64_t min_size = (int64_t)(block / std::max(group_lanes[m], 1)) * kMinTrajPerGroup;
+    k = std::min<int64_t>(k, std::max<int64_t>(1, n_traj[m] / std::max<int64_t>(min_size, 1)));
+    const int64_t per = (n_traj[m] + k - 1) / k;
+    for (int64_t t0 = 0; t0 < n_traj[m]; t0 += per) {
+      BatchItem it;
+      it.mol = (int32_t)m;
+      it.pad = 0;
+      it.t0 = t0;
+      it.t1 = std::min<int64_t>(n_traj[m], t0 + per);
+      items.push_back(it);
+    }
+  }
+  std::stable_sort(items.begin(), items.end(), [&](const BatchItem &x, const BatchItem &y) {
+    const double cx = (double)n_atoms[x.mol] * (double)(x.t1 - x.t0);
+    const double cy = (double)n_atoms[y.mol] * (double)(y.t1 - y.t0);
+    return cx > cy;
+  });
 }
 
 // Lanes per trajectory for a molecule: the tuned value of its size class if
@@ -147,25 +183,13 @@ cosims_status prepare(cosims_batch *b, const uint64_t *seed, const int64_t *firs
     total += n_traj[m];
   }
   if (total > INT32_MAX) return fail(COSIMS_ERR_UNSUPPORTED, "at most 2^31-1 trajectories per run");
-  b->items.clear();
-  std::vector<double> cost;
+  std::vector<int64_t> nt(b->n_mol);
+  std::vector<int> lanes(b->n_mol);
   for (int m = 0; m < b->n_mol; m++) {
-    const BatchMol &bm = b->mols[m];
-    const int64_t per = (int64_t)(kBatchBlock / bm.group_lanes) * kTrajPerGroupPerItem;
-    for (int64_t t0 = 0; t0 < bm.n_traj; t0 += per) {
-      BatchItem it;
-      it.mol = m;
-      it.pad = 0;
-      it.t0 = t0;
-      it.t1 = std::min<int64_t>(bm.n_traj, t0 + per);
-      b->items.push_back(it);
-    }
+    nt[m] = b->mols[m].n_traj;
+    lanes[m] = b->mols[m].group_lanes;
   }
-  std::stable_sort(b->items.begin(), b->items.end(), [&](const BatchItem &x, const BatchItem &y) {
-    const double cx = (double)b->n_atoms[x.mol] * (double)(x.t1 - x.t0);
-    const double cy = (double)b->n_atoms[y.mol] * (double)(y.t1 - y.t0);
-    return cx > cy;
-  });
+  balanced_items(nt, b->n_atoms, lanes, b->block, b->grid, b->items);
   *total_out = total;
   return COSIMS_OK;
 }
@@ -389,9 +413,11 @@ cosims_status cosims_batch_autotune(cosims_batch *b, void *stream) {
     const int slots = b->mols[m].img32.n_slots;
     float best = 1e30f;
     int best_lanes = b->mols[m].group_lanes;
-    // about four million pair terms per evaluation run; lanes that leave each
-    // lane between 8 and 256 atom slots (fewer is all overhead, more is all tail)
-    const int64_t trials = std::min<int64_t>(16384, std::max<int64_t>(2048, (4 << 20) / slots));
+    // about fifty million atom-trajectories per trial (some 50 ms), so that
+    // throughput, not the single longest trajectory, decides; lanes that
+    // leave each lane between 8 and 256 atom slots
+    const int64_t trials =
+        std::min<int64_t>(200000, std::max<int64_t>(4096, (int64_t)50000000 / slots));
     bool warmed = false;
     for (int lanes : {2, 4, 8, 16, 32}) {
       if (slots / lanes > 256 && lanes != 32) continue;
@@ -431,7 +457,11 @@ cosims_status cosims_batch_get_launch(const cosims_batch *b, int32_t mol, int32_
   if (!b || mol < 0 || mol >= b->n_mol) return fail(COSIMS_ERR_INVALID, "bad batch or molecule");
   const int lanes = b->mols[mol].group_lanes;
   if (group_lanes) *group_lanes = lanes;
-  if (item_traj) *item_traj = (kBatchBlock / lanes) * kTrajPerGroupPerItem;
+  if (item_traj) {   // trajectories in the molecule's first item of the last run
+    *item_traj = 0;
+    for (const BatchItem &it : b->items)
+      if (it.mol == mol) { *item_traj = (int32_t)(it.t1 - it.t0); break; }
+  }
   return COSIMS_OK;
 }
 

@@ -27,6 +27,9 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
                   HostImage &h32);
 int mode_stride_for(const MolImage &img);
 size_t batch_mol_smem(BatchMol &bm, int block, int budget, uint32_t img_cap);
+void balanced_items(const std::vector<int64_t> &n_traj, const std::vector<int> &n_atoms,
+                    const std::vector<int> &group_lanes, int block, int grid,
+                    std::vector<BatchItem> &items);
 cosims_status shape_for(bool plain, const MolImage &img, int G, int block_threads,
                         int wide_lanes, int force_type, int sm_count, int max_smem, int64_t n,
                         LaunchShape &ls);

@@ -238,22 +238,24 @@ cosims_status cosims_serve_step(cosims_server *s, void *stream, int32_t *n_finis
       return fail(COSIMS_ERR_UNSUPPORTED, "job %lld needs %zu bytes of shared memory",
                   (long long)j.id, need);
     smem = std::max(smem, need);
-    const int64_t per = (int64_t)(kServeBlock / bm.group_lanes) * 16;
-    for (int64_t t0 = 0; t0 < bm.n_traj; t0 += per) {
-      BatchItem it;
-      it.mol = (int32_t)k;
-      it.pad = 0;
-      it.t0 = t0;
-      it.t1 = std::min<int64_t>(bm.n_traj, t0 + per);
-      items.push_back(it);
-    }
     base += bm.n_traj;
     mols.push_back(bm);
     slots.push_back(j.rounds == 0 ? -j.slot - 1 : j.slot);
   }
-  std::stable_sort(items.begin(), items.end(), [&](const BatchItem &x, const BatchItem &y) {
-    return (double)act[x.mol]->n_atoms * (x.t1 - x.t0) > (double)act[y.mol]->n_atoms * (y.t1 - y.t0);
-  });
+  int per_sm = 1;
+  int orc = batch_occupancy(kServeBlock, smem, &per_sm);
+  if (orc != 0) return cuda_fail((cudaError_t)orc, "round occupancy");
+  per_sm = std::max(1, per_sm);
+  {
+    std::vector<int64_t> nt;
+    std::vector<int> na, lanes;
+    for (size_t k = 0; k < act.size(); k++) {
+      nt.push_back(mols[k].n_traj);
+      na.push_back(act[k]->n_atoms);
+      lanes.push_back(mols[k].group_lanes);
+    }
+    balanced_items(nt, na, lanes, kServeBlock, per_sm * s->sm_count, items);
+  }
   if ((int64_t)items.size() > s->items_cap) {
     cudaFree(s->d_items);
     s->d_items = nullptr;
@@ -273,8 +275,7 @@ cosims_status cosims_serve_step(cosims_server *s, void *stream, int32_t *n_finis
     e = cudaMemsetAsync(s->d_ctrl, 0, sizeof(unsigned long long) * (1 + C_COUNT), st);
   if (e != cudaSuccess) return cuda_fail(e, "round descriptors");
   int rc = batch_sample_launch(s->d_mols, n, base, s->d_pos0, s->d_vel0, s->d_hit, st);
-  int per_sm = 1;
-  if (rc == 0) rc = batch_occupancy(kServeBlock, smem, &per_sm);
+
   BatchArgs a;
   std::memset(&a, 0, sizeof a);
   a.mols = s->d_mols;
@@ -288,7 +289,7 @@ cosims_status cosims_serve_step(cosims_server *s, void *stream, int32_t *n_finis
   a.out = s->d_out;
   a.item_queue = s->d_ctrl;
   a.counters = s->d_ctrl + 1;
-  if (rc == 0) rc = batch_launch(a, kServeBlock, std::max(1, per_sm) * s->sm_count, smem, st);
+  if (rc == 0) rc = batch_launch(a, kServeBlock, per_sm * s->sm_count, smem, st);
   if (rc == 0) rc = batch_reduce_launch(s->d_mols, n, s->d_out, 0, s->d_round, st);
   if (rc != 0) return cuda_fail((cudaError_t)rc, "round launch");
   accumulate_sums<<<(n + 127) / 128, 128, 0, st>>>(s->d_round, s->d_slots, n, s->d_running);

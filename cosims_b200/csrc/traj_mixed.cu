@@ -7,16 +7,97 @@ namespace mixed {
 
 // ---- batched form: one persistent launch over many molecules ------------------
 // CTAs take work items (a molecule and a range of its trajectories) from a
-// device queue.  When an item's molecule differs from the one staged, the CTA
-// waits for its groups, then bulk-copies the new image into shared memory
-// (molecules over the launch's shared-memory budget are read through L1/L2).
-// Groups then take the item's trajectories from a shared-memory counter.
-// One work item of the batched kernel.  Not inlined: each (variant, staging)
-// pair gets its own register allocation instead of the union of all six.
+// device queue.  A CTA keeps one molecule staged in shared memory (molecules
+// over the launch's shared-memory budget are read through L1/L2) and its
+// groups draw trajectories from the current item; the group that finds the
+// item used up fetches the next one.  While the next item is of the same
+// molecule the groups go straight on; only an item of another molecule makes
+// the CTA wait for its groups and restage.  Items of one molecule are adjacent
+// in the queue (sorted by cost), so a CTA rarely restages.
+
+// CTA-shared state of the current molecule.
+struct BatchShared {
+  unsigned long long state;   // (item << 32) | next trajectory of the item; kNoItem: none
+  int fetch_lock;             // held by the group fetching the next item
+  int pending;                // item of another molecule to stage next, -1: none
+  int staged;                 // molecule in shared memory, -1: none
+};
+constexpr unsigned long long kNoItem = 0xffffffffull << 32;
+
+struct BatchSource {
+  const BatchArgs *a;
+  BatchShared *sh;
+  int mol;                    // the staged molecule
+  long long base;             // its first slot in the batch arrays
+};
+__device__ __forceinline__ cosims_traj_out *out_of(const BatchSource &s) { return s.a->out; }
+__device__ __forceinline__ long long budget_of(const BatchSource &) { return 0; }
+__device__ __forceinline__ bool park(const BatchSource &, NarrowLanes &, GroupState &) {
+  return false;
+}
+
+// Next trajectory of the staged molecule for a group; false when the
+// molecule has no more items (the CTA then restages or stops).
+__device__ __forceinline__ bool acquire(const BatchSource &src, const DevParams &p,
+                                        NarrowLanes &ln, GroupState &GS) {
+  const BatchArgs &A = *src.a;
+  BatchShared &sh = *src.sh;
+  for (;;) {
+    long long slot = -1;
+    if (ln.lane == 0) {
+      bool gave_up = true;
+      for (uint32_t spin = 0; spin < kHandoffSpinLimit; ++spin) {
+        const unsigned long long w = atomicAdd(&sh.state, 0ull);
+        if (w == kNoItem) { gave_up = false; break; }
+        const int item = (int)(w >> 32);
+        const long long t = (long long)(uint32_t)w;
+        const BatchItem it = A.items[item];
+        if (t < it.t1 - it.t0) {
+          if (atomicCAS(&sh.state, w, w + 1) == w) {
+            slot = src.base + it.t0 + t;
+            gave_up = false;
+            break;
+          }
+          continue;
+        }
+        // the item is used up: one group fetches the next, the others retry
+        if (atomicCAS(&sh.fetch_lock, 0, 1) == 0) {
+          if (atomicAdd(&sh.state, 0ull) == w) {
+            const unsigned long long nxt = atomicAdd(A.item_queue, 1ull);
+            if (nxt < (unsigned long long)A.n_items && A.items[nxt].mol == src.mol) {
+              atomicExch(&sh.state, nxt << 32);
+            } else {
+              if (nxt == (unsigned long long)A.n_items) mark_first(A.counters, C_T_DRAIN_INV);
+              sh.pending = nxt < (unsigned long long)A.n_items ? (int)nxt : -1;
+              __threadfence_block();
+              atomicExch(&sh.state, kNoItem);
+            }
+          }
+          atomicExch(&sh.fetch_lock, 0);
+        }
+      }
+      if (gave_up) atomicOr(A.counters + C_ERROR, 2ull);
+    }
+    slot = __shfl_sync(ln.gmask, slot, 0, ln.G);
+    if (slot < 0) return false;
+    if (!A.hit[slot]) {                       // ellipsoid miss: chi = 0
+      if (ln.lane == 0) {
+        cosims_traj_out o = {0.0, 0.0, 0, 0u};
+        A.out[slot] = o;
+      }
+      continue;
+    }
+    traj_begin(GS.s, slot, A.pos0 + 3 * slot, A.vel0 + 3 * slot, p.dt, false);
+    return true;
+  }
+}
+
+// The groups of a CTA on one staged molecule until its items run out.  Not
+// inlined: each (variant, staging) pair gets its own register allocation
+// instead of the union of all six.
 template <int TYPE, bool SMEM>
-__device__ __noinline__ void batch_item(const BatchMol &bm, unsigned char *smem,
-                                        const BatchArgs &a, const BatchItem &it,
-                                        unsigned long long *q) {
+__device__ __noinline__ void batch_session(const BatchMol &bm, unsigned char *smem,
+                                           const BatchArgs &a, BatchShared *sh, int mol) {
   const unsigned char *base = SMEM ? smem : bm.img32.gbase;
   const View m = make_view(base, bm.img32);
   const View64 m64 = make_view64(bm.img64);
@@ -34,12 +115,7 @@ __device__ __noinline__ void batch_item(const BatchMol &bm, unsigned char *smem,
     if (Traits<TYPE>::kClusters) modes[m.nc] = 0;
   }
   __syncwarp();
-  const long long b = bm.base + it.t0;
-  MainSource src;
-  src.pos0 = a.pos0 + 3 * b; src.vel0 = a.vel0 + 3 * b; src.hit = a.hit + b;
-  src.order = nullptr; src.n = it.t1 - it.t0;
-  src.out = a.out + b; src.queue = q; src.counters = nullptr;
-  src.ho = Handoff{};
+  const BatchSource src{&a, sh, mol, bm.base};
   Tally tl;
   group_loop<TYPE>(m, m64, bm.par, ln, modes, *S, src, tl);
   fold_tally<TYPE>(*S, tl);
@@ -48,38 +124,35 @@ __device__ __noinline__ void batch_item(const BatchMol &bm, unsigned char *smem,
 }
 
 template <int TYPE>
-__device__ __forceinline__ void batch_item_s(const BatchMol &bm, unsigned char *smem,
-                                             const BatchArgs &a, const BatchItem &it,
-                                             unsigned long long *q) {
-  if (bm.use_smem) batch_item<TYPE, true>(bm, smem, a, it, q);
-  else batch_item<TYPE, false>(bm, smem, a, it, q);
+__device__ __forceinline__ void batch_session_s(const BatchMol &bm, unsigned char *smem,
+                                                const BatchArgs &a, BatchShared *sh, int mol) {
+  if (bm.use_smem) batch_session<TYPE, true>(bm, smem, a, sh, mol);
+  else batch_session<TYPE, false>(bm, smem, a, sh, mol);
 }
 
 __global__ void __launch_bounds__(kBatchMaxBlock, 1) batch_mixed_kernel(const BatchArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
   __shared__ BatchMol cur;
-  __shared__ int s_item, s_mol;
-  __shared__ unsigned long long s_queue;
+  __shared__ BatchShared sh;
   if (threadIdx.x == 0) {
-    s_mol = -1;
     mark_first(a.counters, C_T_START_INV);
+    const unsigned long long first = atomicAdd(a.item_queue, 1ull);
+    if (first == (unsigned long long)a.n_items) mark_first(a.counters, C_T_DRAIN_INV);
+    sh.pending = first < (unsigned long long)a.n_items ? (int)first : -1;
+    sh.staged = -1;
   }
   uint32_t stagings = 0;
   for (;;) {
-    if (threadIdx.x == 0) s_item = (int)atomicAdd(a.item_queue, 1ull);
     __syncthreads();
-    const int item = s_item;
-    if (item >= a.n_items) {
-      if (threadIdx.x == 0 && item == a.n_items) mark_first(a.counters, C_T_DRAIN_INV);
-      break;
-    }
-    const BatchItem it = a.items[item];
-    if (it.mol != s_mol) {
+    const int item = sh.pending;
+    if (item < 0) break;
+    const int mol = a.items[item].mol;
+    if (mol != sh.staged) {
       __syncthreads();
       if (threadIdx.x == 0) {
-        cur = a.mols[it.mol];
-        s_mol = it.mol;
+        cur = a.mols[mol];
+        sh.staged = mol;
       }
       __syncthreads();
       if (cur.use_smem) {
@@ -91,17 +164,20 @@ __global__ void __launch_bounds__(kBatchMaxBlock, 1) batch_mixed_kernel(const Ba
         stagings++;
       }
     }
-    if (threadIdx.x == 0) s_queue = 0ull;
+    if (threadIdx.x == 0) {
+      sh.state = (unsigned long long)item << 32;
+      sh.fetch_lock = 0;
+      sh.pending = -1;
+    }
     __syncthreads();
     switch (cur.type) {
-      case 1: batch_item_s<1>(cur, smem, a, it, &s_queue); break;
-      case 2: batch_item_s<2>(cur, smem, a, it, &s_queue); break;
-      case 3: batch_item_s<3>(cur, smem, a, it, &s_queue); break;
-      case 4: batch_item_s<4>(cur, smem, a, it, &s_queue); break;
-      case 5: batch_item_s<5>(cur, smem, a, it, &s_queue); break;
-      default: batch_item_s<6>(cur, smem, a, it, &s_queue); break;
+      case 1: batch_session_s<1>(cur, smem, a, &sh, mol); break;
+      case 2: batch_session_s<2>(cur, smem, a, &sh, mol); break;
+      case 3: batch_session_s<3>(cur, smem, a, &sh, mol); break;
+      case 4: batch_session_s<4>(cur, smem, a, &sh, mol); break;
+      case 5: batch_session_s<5>(cur, smem, a, &sh, mol); break;
+      default: batch_session_s<6>(cur, smem, a, &sh, mol); break;
     }
-    __syncthreads();   // every group is done with the item before a restage
   }
   if (threadIdx.x == 0) mark_last(a.counters, C_T_END);
 }

@@ -301,6 +301,9 @@ cosims_status cosims_batch_run(cosims_batch *b, const uint64_t *seed,
 cosims_status cosims_batch_run_async(cosims_batch *b, const uint64_t *seed,
                                      const int64_t *first_index, const int64_t *n_traj,
                                      cosims_ccs_sums *d_sums, void *stream);
+/* Lanes per trajectory of molecule mol, and the trajectories in its first
+ * work item of the last run (items are cut to about equal cost, about three
+ * per CTA; 0 before a run). */
 cosims_status cosims_batch_get_launch(const cosims_batch *b, int32_t mol,
                                       int32_t *group_lanes, int32_t *item_traj);
 /* Progress interval for the per-molecule n_eff bookkeeping (as update_every
