@@ -95,13 +95,13 @@ __device__ __forceinline__ bool acquire(const BatchSource &src, const DevParams 
 // The groups of a CTA on one staged molecule until its items run out.  Not
 // inlined: each (variant, staging) pair gets its own register allocation
 // instead of the union of all six.
-template <int TYPE, bool SMEM>
+template <int TYPE, bool SMEM, int GT>
 __device__ __noinline__ void batch_session(const BatchMol &bm, unsigned char *smem,
                                            const BatchArgs &a, BatchShared *sh, int mol) {
   const unsigned char *base = SMEM ? smem : bm.img32.gbase;
   const View m = make_view(base, bm.img32);
   const View64 m64 = make_view64(bm.img64);
-  const int G = bm.group_lanes;
+  const int G = GT > 0 ? GT : bm.group_lanes;
   GroupState *S;
   uint8_t *modes;
   narrow_scratch(smem, SMEM ? bm.img32.bytes : 0u, G, bm.mode_stride, S, modes);
@@ -123,11 +123,24 @@ __device__ __noinline__ void batch_session(const BatchMol &bm, unsigned char *sm
   if (ln.lane == 0) flush_group<TYPE>(*S, m64.n, a.counters);
 }
 
+// lanes per trajectory fixed at compile time for 8, 16 and 32 (as the
+// single-molecule kernels); other counts at run time
+template <int TYPE, bool SMEM>
+__device__ __forceinline__ void batch_session_g(const BatchMol &bm, unsigned char *smem,
+                                                const BatchArgs &a, BatchShared *sh, int mol) {
+  switch (bm.group_lanes) {
+    case 8: batch_session<TYPE, SMEM, 8>(bm, smem, a, sh, mol); break;
+    case 16: batch_session<TYPE, SMEM, 16>(bm, smem, a, sh, mol); break;
+    case 32: batch_session<TYPE, SMEM, 32>(bm, smem, a, sh, mol); break;
+    default: batch_session<TYPE, SMEM, 0>(bm, smem, a, sh, mol); break;
+  }
+}
+
 template <int TYPE>
 __device__ __forceinline__ void batch_session_s(const BatchMol &bm, unsigned char *smem,
                                                 const BatchArgs &a, BatchShared *sh, int mol) {
-  if (bm.use_smem) batch_session<TYPE, true>(bm, smem, a, sh, mol);
-  else batch_session<TYPE, false>(bm, smem, a, sh, mol);
+  if (bm.use_smem) batch_session_g<TYPE, true>(bm, smem, a, sh, mol);
+  else batch_session_g<TYPE, false>(bm, smem, a, sh, mol);
 }
 
 __global__ void __launch_bounds__(kBatchMaxBlock, 1) batch_mixed_kernel(const BatchArgs a) {
