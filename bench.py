@@ -479,6 +479,119 @@ def serving_workload(args, rank, world, local, dist, torch):
     print(json.dumps(line))
 
 
+def molecule_workload(args, rank, world, local, dist, torch):
+    """Configurations 2 and 0 as single-molecule integrals.
+
+    protein (configuration 2): 3000-atom ion, charge +10, partial charges
+    N(0, 0.35 e), the PCM far-field approximation beyond 12 A (force variant 1);
+    one step = one integral of 1e6 trajectories in the mixed form; the CCS
+    error against the plain FP64 form is taken on the first 1e4 of them.
+    small (configuration 0): neutral 128-atom molecule (variant 5); one step =
+    one integral of 1e4 trajectories in the plain FP64 form (the drop-in)."""
+    import numpy as np
+    from cosims_b200 import abi, engine, host, shard, synth
+    protein = args.workload == "protein"
+    mol_ = synth.config2_molecule() if protein else synth.config0_molecule()
+    force = "multipole12" if protein else "cutoff"
+    n_traj = 1_000_000 if protein else 10_000
+    form = abi.MIXED if protein else abi.PLAIN_F64
+    tmp = tempfile.mkdtemp(prefix="cosims_bench_")
+    mp_, ip = synth.write_case(tmp, mol_, force, traj_thousands=n_traj / 1000, iterations=1)
+    st = host.setup_from_files(mp_, ip, seed=SEED, device=local)
+    mol, par = st.mol, st.params
+    stream = torch.cuda.current_stream()
+    d = torch.zeros(1024, dtype=torch.uint8, device="cuda")
+    sz = abi.C.sizeof(abi.CcsSums)
+    step_sums = torch.zeros((args.steps, 128), dtype=torch.uint8, device="cuda")
+    flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    first0 = shard.first_index(rank)
+    ctx = engine.Context(mol, par, form, device=local)
+    g = None
+    if form == abi.MIXED:
+        best = (1e30, None)
+        for lanes in (16, 32):
+            ctx.set_launch(group_lanes=lanes)
+            ctx.run_sampled_device(SEED + 7, 0, n_traj // 10, 0, d.data_ptr(), stream)
+            best = min(best, (ctx.kernel_ms(), lanes))
+        g = best[1]
+        ctx.set_launch(group_lanes=g)
+    for w in range(args.warmup):
+        ctx.run_sampled_device(SEED, first0 + w * n_traj, n_traj, 0, d.data_ptr(), stream)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms, kern = [], []
+    for k in range(args.steps):
+        flush.zero_()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx.run_sampled_device(SEED, first0 + (args.warmup + k) * n_traj, n_traj, 0,
+                               step_sums[k].data_ptr(), stream)
+        e.record(stream)
+        torch.cuda.synchronize()
+        ms.append(a.elapsed_time(e))
+        kern.append(ctx.kernel_ms())
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    mean_ms = shard.max_over_ranks(sum(ms) / len(ms), dist, "cuda")
+    value = world * n_traj / (mean_ms / 1000.0)
+    raw = step_sums.cpu().numpy()
+    sums = [abi.CcsSums.from_buffer_copy(raw[k, :sz].tobytes()) for k in range(args.steps)]
+    pot_flops = FLOPS_POT_CHARGED if par.charged else FLOPS_POT_NEUTRAL
+    flops = [FLOPS_LJ * x.pair_lj + FLOPS_ES * x.pair_es + FLOPS_FAR * x.far_terms +
+             pot_flops * x.pair_pot for x in sums]
+    kmean = sum(kern) / len(kern)
+    achieved = sum(flops) / len(flops) / (kmean / 1000.0) / 1e12
+    fp32_peak, fp64_peak = engine.probe_peaks(local)
+    peak = fp32_peak if form == abi.MIXED else fp64_peak
+    merged = shard.merge_sums(sums, dist, "cuda")
+    # the other form on the first 1e4 trajectories of the first timed integral
+    n_cmp = 10_000
+    other = engine.Context(mol, par, abi.PLAIN_F64 if form == abi.MIXED else abi.MIXED,
+                           device=local)
+    first_cmp = first0 + args.warmup * n_traj
+    other.run_sampled_device(SEED, first_cmp, n_cmp, 0, d.data_ptr(), stream)
+    so = abi.CcsSums.from_buffer_copy(d.cpu().numpy()[:sz].tobytes())
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    ctx.run_sampled_device(SEED, first_cmp, n_cmp, 0, d.data_ptr(), stream)
+    e.record(stream)
+    torch.cuda.synchronize()
+    sf = abi.CcsSums.from_buffer_copy(d.cpu().numpy()[:sz].tobytes())
+    plain_sum = so.sum if protein else sf.sum
+    err = abs(sf.sum - so.sum) / plain_sum * 100.0
+    other.close()
+    ctx.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32 pair forces / fp64 integration" if protein else "f64",
+            "data": "synthetic",
+            "config": {"workload": (f"3000-atom synthetic ion, charge +10, force variant "
+                                    f"{par.force_type} (PCM far field beyond 12 A), mixed form, "
+                                    f"{n_traj} trajectories per step") if protein else
+                       (f"neutral 128-atom synthetic molecule, force variant {par.force_type}, "
+                        f"plain FP64 form, {n_traj} trajectories per step"),
+                       "atoms": int(mol.n_atoms), "group_lanes": g,
+                       "l2": "flushed between steps (512 MiB write)"},
+            "ccs": {"omega_A2": merged["omega"], "se_A2": merged["se"],
+                    "err_pct_mixed_vs_plain": err, "compared_trajectories": n_cmp,
+                    "bar_pct": 0.3},
+            "roofline": {"bound": "fp32" if protein else "fp64", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "kernel": f"traj_{'mixed' if protein else 'plain'}_kernel",
+                         "kernel_ms": kmean},
+            "clocks": clk,
+        }
+        print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -491,9 +604,12 @@ def main():
                          "of one form only, no L2 flush buffer, no sweep")
     ap.add_argument("--profile-traj", type=int, default=20000)
     ap.add_argument("--group-lanes", type=int, default=0)
-    ap.add_argument("--workload", choices=["integral", "batched", "serving"], default="integral",
+    ap.add_argument("--workload", choices=["integral", "batched", "serving", "protein", "small"],
+                    default="integral",
                     help="integral: the 512-atom ion (default line); batched: 256 molecules "
-                         "in one persistent launch; serving: Poisson stream of CCS requests")
+                         "in one persistent launch; serving: Poisson stream of CCS requests; "
+                         "protein: the 3000-atom ion, 1e6 trajectories, mixed form; small: the "
+                         "neutral 128-atom molecule, 1e4 trajectories, plain FP64 form")
     ap.add_argument("--molecules", type=int, default=256, help="batched/serving: library size")
     ap.add_argument("--rate", type=float, default=50.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
@@ -521,6 +637,9 @@ def main():
         return
     if args.workload == "serving":
         serving_workload(args, rank, world, local, dist, torch)
+        return
+    if args.workload in ("protein", "small"):
+        molecule_workload(args, rank, world, local, dist, torch)
         return
 
     tmp = tempfile.mkdtemp(prefix="cosims_bench_")

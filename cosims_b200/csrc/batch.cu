@@ -43,7 +43,7 @@ int size_class(int n_atoms) {
 // Sets bm.use_smem and bm.mode_stride.
 size_t batch_mol_smem(BatchMol &bm, int block, int budget, uint32_t img_cap) {
   bm.use_smem = bm.img32.bytes <= img_cap ? 1 : 0;
-  bm.mode_stride = mode_stride_for(bm.img32);
+  bm.mode_stride = mode_stride_for(bm.img32, bm.type);
   const size_t groups = (size_t)(block / bm.group_lanes);
   const size_t scratch = groups * ((size_t)kGroupStateBytes + (size_t)bm.mode_stride);
   size_t need = (bm.use_smem ? ((bm.img32.bytes + 15u) & ~15u) : 0) + scratch;

@@ -252,9 +252,13 @@ static cosims_status grow(T **p, int64_t *cap, int64_t need) {
 // Shared-memory bytes of one mixed-form group: its trajectory state and its
 // cluster-mode scratch (n_clusters + 1 bytes: the last entry, always 0,
 // belongs to the pad atoms).
-int mode_stride_for(const MolImage &img) {
+int mode_stride_for(const MolImage &img, int force_type) {
   if (!img.uses_clusters) return 0;
-  int s = (img.n_clusters + 1 + 3) & ~3;
+  // variants 1, 2, 5 keep a 4-byte entry per cluster (the list of clusters
+  // that add pair terms); the others one mode byte per cluster, plus the pad
+  // atoms' cluster
+  const int per = (force_type == 1 || force_type == 2 || force_type == 5) ? 4 : 1;
+  int s = ((img.n_clusters + 1) * per + 3) & ~3;
   if (((s / 4) & 1) == 0) s += 4;     // odd word count: groups hit distinct banks
   return s;
 }
@@ -268,7 +272,7 @@ cosims_status shape_for(bool plain, const MolImage &img, int G, int block_thread
                         int wide_lanes, int force_type, int sm_count, int max_smem, int64_t n,
                         LaunchShape &ls) {
   const int budget = max_smem - 1024;
-  const int stride = plain ? 0 : mode_stride_for(img);
+  const int stride = plain ? 0 : mode_stride_for(img, force_type);
   const size_t per_group = plain ? 0 : (size_t)kGroupStateBytes + (size_t)stride;
   const size_t per_wide = (!plain && wide_lanes > 0) ? wide_group_bytes(wide_lanes, stride) : 0;
   const size_t img_bytes = (img.bytes + 15u) & ~15u;

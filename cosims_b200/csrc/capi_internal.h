@@ -25,7 +25,7 @@ cosims_status validate(const cosims_molecule *mol, const cosims_params *par);
 DevParams make_dev_params(const cosims_params *p);
 void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h64,
                   HostImage &h32);
-int mode_stride_for(const MolImage &img);
+int mode_stride_for(const MolImage &img, int force_type);
 size_t batch_mol_smem(BatchMol &bm, int block, int budget, uint32_t img_cap);
 void balanced_items(const std::vector<int64_t> &n_traj, const std::vector<int> &n_atoms,
                     const std::vector<int> &group_lanes, int block, int grid,

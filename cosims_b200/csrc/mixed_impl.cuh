@@ -68,8 +68,12 @@ struct Traits {
   // pair terms per evaluation depend on the position (far clusters, cut-off
   // without a charge field); for 3, 4 and 6 they are n_atoms every time
   static constexpr bool kVaryingPairs = TYPE == 1 || TYPE == 2 || TYPE == 5;
-  // the per-cluster decision is one bit (the LJ cut-off)
-  static constexpr bool kMaskable = TYPE == 3 || TYPE == 5;
+  // the per-cluster decision is one bit (the LJ cut-off) and every atom adds
+  // a charge field, so all slots are evaluated with a register cut-off mask
+  static constexpr bool kMaskable = TYPE == 3;
+  // clusters with nothing to add are common (far field, cut-off): pass 2
+  // walks a list of the clusters that add something
+  static constexpr bool kListed = TYPE == 1 || TYPE == 2 || TYPE == 5;
   static constexpr bool kCharge = TYPE <= 4;
   static constexpr bool kFar = TYPE == 1 || TYPE == 2;
   // every atom carries the charge field (types 3, 4): no per-pair branch
@@ -233,6 +237,58 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
       pair<TYPE>(m, a0, b0, m0, hx, hy, hz, lx, ly, lz, s);
       pair<TYPE>(m, a1, b1, m1, hx, hy, hz, lx, ly, lz, s);
     }
+  } else if (Traits<TYPE>::kListed) {
+    // pass 1: near/far decision per cluster (FP64), far-field terms; the
+    // clusters that add pair terms go into the group's list (cluster << 8 |
+    // mode), compacted by ballot, so pass 2 skips the rest as the reference
+    // does (forceAccel.cpp:221-633, 807-854)
+    uint32_t *list = reinterpret_cast<uint32_t *>(modes);
+    const int gbase = (threadIdx.x & 31) & ~(G - 1);
+    const unsigned gbits = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
+    int count = 0;
+    for (int c0 = 0; c0 < m.nc; c0 += G) {
+      const int c = c0 + lane;
+      uint32_t mode = 0;
+      if (c < m.nc) {
+        const ClusterF32 &C = m.cl[c];
+        const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
+        const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+        const bool in_disp = !(r2 > C.dr2);
+        if (TYPE == 5) {
+          mode = in_disp ? M_LJ : 0;
+        } else if (r2 > C.mpr2) {
+          far_terms(m, c, p.multipole_order, (float)d0, (float)d1, (float)d2, s);
+          w.far++;
+          mode = TYPE == 2 ? M_LJ : (in_disp ? M_LJQ : 0);
+        } else {
+          mode = M_ES | ((TYPE == 2 || in_disp) ? M_LJ : 0);
+        }
+        const uint32_t cnt = (uint32_t)(C.a1 - C.a0);
+        if (mode & M_ES) w.es += cnt;
+        else if (mode) w.lj += cnt;
+      }
+      const unsigned mine = (__ballot_sync(0xffffffffu, mode != 0) >> gbase) & gbits;
+      if (mode != 0) list[count + __popc(mine & ((1u << lane) - 1u))] = ((uint32_t)c << 8) | mode;
+      count += __popc(mine);
+    }
+    ln.sync();
+    // pass 2: the listed clusters' atoms; with 32 lanes two clusters at a time
+    // (clusters hold at most a few tens of atoms)
+    const int split = G == 32 ? 16 : G;
+    const int sub = lane & (split - 1), half = G == 32 ? (lane >> 4) : 0;
+    const int step = G == 32 ? 2 : 1;
+    for (int i = half; i - half < count; i += step) {
+      if (i < count) {
+        const uint32_t e = list[i];
+        const ClusterF32 &C = m.cl[e >> 8];
+        const uint32_t mode = e & 0xffu;
+        for (int k = C.a0 + sub; k < C.a1; k += split) {
+          const float4 a = m.a4[k], b = m.b4[k];
+          pair<TYPE>(m, a, b, mode, hx, hy, hz, lx, ly, lz, s);
+        }
+      }
+    }
+    ln.sync();
   } else if (Traits<TYPE>::kClusters) {
     // pass 1: near/far decision per cluster (FP64), far-field terms
     for (int c = lane; c < m.nc; c += G) {
