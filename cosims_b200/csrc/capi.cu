@@ -186,10 +186,23 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   i64.off[S_ATOMS] = b64.add(a64.data(), sizeof(AtomF64) * n);
   i64.off[S_PERM] = b64.add(perm.data(), 4 * n);
   i64.off[S_CLUSTERS] = b64.add(c64.data(), sizeof(ClusterF64) * nc);
+  // event slots of the plain form's exact wide phase, in the serial order
+  std::vector<int32_t> slots;
+  const bool far_events = p->force_type == 1 || p->force_type == 2;
+  if (uses) {
+    for (int c = 0; c < nc; c++) {
+      if (far_events)                  // the far field's three parts, in order
+        for (int part = 0; part < 3; part++) { slots.push_back(-1 - part); slots.push_back(c); }
+      for (int k = coff[c]; k < coff[c + 1]; k++) { slots.push_back(k); slots.push_back(c); }
+    }
+  } else {
+    for (int k = 0; k < n; k++) { slots.push_back(k); slots.push_back(0); }
+  }
+  i64.off[S_SLOTS] = b64.add(slots.data(), 4 * slots.size());
   b64.finish();
   i64.bytes = (uint32_t)b64.buf.size();
   i64.n_atoms = n;
-  i64.n_slots = n;
+  i64.n_slots = (int)(slots.size() / 2);      // exact-phase events
   i64.n_clusters = nc;
   i64.uses_clusters = uses ? 1 : 0;
   h64.bytes = std::move(b64.buf);
@@ -274,7 +287,9 @@ cosims_status shape_for(bool plain, const MolImage &img, int G, int block_thread
   const int budget = max_smem - 1024;
   const int stride = plain ? 0 : mode_stride_for(img, force_type);
   const size_t per_group = plain ? 0 : (size_t)kGroupStateBytes + (size_t)stride;
-  const size_t per_wide = (!plain && wide_lanes > 0) ? wide_group_bytes(wide_lanes, stride) : 0;
+  const size_t per_wide = wide_lanes <= 0 ? 0
+                         : plain ? exact_scratch_bytes(force_type, img.n_clusters)
+                                 : wide_group_bytes(wide_lanes, stride);
   const size_t img_bytes = (img.bytes + 15u) & ~15u;
   int cands[4] = {block_threads, 0, 0, 0};
   int ncand = 1;
@@ -296,9 +311,17 @@ cosims_status shape_for(bool plain, const MolImage &img, int G, int block_thread
       bool ok = true;
       for (;;) {
         size_t scratch = (size_t)(block / G) * per_group;
-        // wide phase: whole wide groups only, at most 15 (named barriers 1..15)
-        t.wide_lanes = (per_wide && block >= wide_lanes && block / wide_lanes <= 15) ? wide_lanes : 0;
-        if (t.wide_lanes) scratch = std::max(scratch, (size_t)(block / wide_lanes) * per_wide);
+        if (plain) {
+          // plain form: one exact wide group per CTA, which must be kPlainBlock threads
+          t.wide_lanes = (per_wide && block == kPlainBlock) ? kPlainBlock : 0;
+          if (t.wide_lanes) scratch = per_wide;
+        } else {
+          // wide phase: whole wide groups only, at most 15 (named barriers 1..15);
+          // threads beyond them sit the phase out
+          t.wide_lanes = (per_wide && block >= wide_lanes) ? wide_lanes : 0;
+          if (t.wide_lanes)
+            scratch = std::max(scratch, (size_t)std::min(block / wide_lanes, 15) * per_wide);
+        }
         size_t smem = (t.use_smem ? img_bytes : 0) + scratch;
         if ((int)smem <= budget) { t.smem = smem; break; }
         if (block <= std::max(G, 32)) { ok = false; break; }
@@ -333,7 +356,8 @@ cosims_status shape_for(bool plain, const MolImage &img, int G, int block_thread
 }
 
 int ctx_wide_lanes(const cosims_ctx *c) {
-  if (c->precision != COSIMS_PRECISION_MIXED || c->ho_budget <= 0) return 0;
+  if (c->ho_budget <= 0) return 0;
+  if (c->precision == COSIMS_PRECISION_PLAIN_F64) return kPlainBlock;   // the whole CTA
   return c->ho_wide > 0 ? c->ho_wide : default_wide_lanes(c->n_atoms);
 }
 
@@ -420,10 +444,8 @@ cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0
   a.out = d_out;
   a.queue = c->d_queue;
   a.counters = c->d_counters;
-  if (!plain) {
-    st = handoff_prepare(c, n, ls, a.ho, s);
-    if (st != COSIMS_OK) return st;
-  }
+  st = handoff_prepare(c, n, ls, a.ho, s);
+  if (st != COSIMS_OK) return st;
   if (!c->ev0) {
     e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
@@ -505,6 +527,7 @@ cosims_status cosims_ctx_create(const cosims_molecule *mol, const cosims_params 
   c->img32 = c->h32.img;
   c->group_lanes = precision == COSIMS_PRECISION_PLAIN_F64 ? 1 : default_group_lanes(mol->n_atoms);
   c->block_threads = precision == COSIMS_PRECISION_PLAIN_F64 ? 128 : 0;   // 0: chosen per run
+  if (precision == COSIMS_PRECISION_PLAIN_F64) c->ho_budget = kDefaultPlainHandoffBudget;
   cudaError_t e = cudaMalloc((void **)&c->d_img64, c->img64.bytes);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_img32, c->img32.bytes);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_queue, sizeof(unsigned long long));
@@ -578,11 +601,13 @@ cosims_status cosims_ctx_kernel_timeline(cosims_ctx *c, double *drain_ms, double
 
 cosims_status cosims_ctx_set_handoff(cosims_ctx *c, int64_t step_budget, int32_t wide_lanes) {
   if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
-  if (c->precision != COSIMS_PRECISION_MIXED)
-    return fail(COSIMS_ERR_INVALID, "the hand-off belongs to the mixed form");
+  const bool plain = c->precision == COSIMS_PRECISION_PLAIN_F64;
+  if (plain && wide_lanes != 0 && wide_lanes != kPlainBlock)
+    return fail(COSIMS_ERR_INVALID, "the plain form's wide group is its %d-thread CTA", kPlainBlock);
   if (wide_lanes < 0 || wide_lanes > 512 || (wide_lanes & 31))
     return fail(COSIMS_ERR_INVALID, "wide_lanes must be 0 or a multiple of 32 up to 512");
-  c->ho_budget = step_budget == 0 ? kDefaultHandoffBudget : (step_budget < 0 ? 0 : step_budget);
+  const int64_t dflt = plain ? kDefaultPlainHandoffBudget : kDefaultHandoffBudget;
+  c->ho_budget = step_budget == 0 ? dflt : (step_budget < 0 ? 0 : step_budget);
   c->ho_wide = wide_lanes;
   return COSIMS_OK;
 }

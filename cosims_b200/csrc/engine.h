@@ -11,7 +11,10 @@
 //     AtomF64 records in "force order" -- cluster by cluster in the
 //     reference's member order for the cluster force variants (1, 2, 3, 5),
 //     file order otherwise; perm[i] = force-order slot of file atom i
-//     (getPotential walks atoms in file order); ClusterF64 records.
+//     (getPotential walks atoms in file order); ClusterF64 records; the event
+//     slots of the exact wide phase, int2 {atom (force order) or -1 for a
+//     cluster's far-field event, cluster}: cluster by cluster, a far-field
+//     slot before each cluster's atoms for variants 1 and 2.
 //   F32 image (mixed form): in force order, two float4 arrays, (x, y, z, q)
 //     and (sigma^6, 24 eps/mu, cluster id as integer bits, 0), so lanes
 //     reading consecutive atoms hit consecutive banks; ClusterF32 records (FP64
@@ -37,7 +40,7 @@ constexpr int kTrajStateBytes = 200;               // one trajectory's integrato
 constexpr int kGroupStateBytes = 240;              // TrajState + a group's counters (shared memory)
 constexpr int kWideSlotFloats = 24;                // per-warp reduction slot of a wide group
 
-enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_LJ, S_COUNT };
+enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_LJ, S_SLOTS, S_COUNT };
 
 struct AtomF64 {            // 56 bytes
   double x, y, z, q, sig6, eps24m, eps4;
@@ -153,6 +156,33 @@ __host__ __device__ inline uint32_t wide_group_bytes(int wide_lanes, int mode_st
   return b;
 }
 constexpr int64_t kDefaultHandoffBudget = 2048;   // steps before a trajectory goes wide
+
+// Plain form: a parked trajectory is finished by a whole CTA (kPlainBlock
+// threads): warps 1..3 evaluate the terms of kExactChunk event slots at a time
+// while warp 0 adds the previous chunk in the reference's order, one
+// accumulator per lane.  Shared memory of that phase: cluster flags, two chunk
+// buffers of [K][kExactRow] doubles (a row padded to an odd count of doubles so
+// that the adding lanes read different banks), K accumulators and a broadcast
+// word.
+constexpr int kPlainBlock = 128;
+constexpr int kExactProducers = kPlainBlock - 32;
+#ifndef COSIMS_EXACT_PER_THREAD
+#define COSIMS_EXACT_PER_THREAD 1
+#endif
+constexpr int kExactPerThread = COSIMS_EXACT_PER_THREAD;
+constexpr int kExactChunk = kExactProducers * kExactPerThread;
+constexpr int kExactRow = kExactChunk + 1;
+constexpr int64_t kDefaultPlainHandoffBudget = 256;
+__host__ __device__ inline int exact_accumulators(int force_type) {
+  return (force_type == 1 || force_type == 2) ? 15 : (force_type == 3 || force_type == 4) ? 12 : 4;
+}
+__host__ __device__ inline uint32_t exact_scratch_bytes(int force_type, int n_clusters) {
+  const uint32_t K = (uint32_t)exact_accumulators(force_type);
+  uint32_t b = ((uint32_t)n_clusters + 15u) & ~15u;                  // cluster flags
+  b += 2u * K * (uint32_t)kExactRow * 8u;                            // chunk buffers
+  b += 16u * 8u + 16u;                                               // accumulators, broadcast
+  return b;
+}
 inline int default_wide_lanes(int n_atoms) { return n_atoms <= 1024 ? 128 : 256; }
 
 struct TrajArgs {

@@ -1060,7 +1060,7 @@ __device__ __noinline__ void wide_phase(unsigned char *smem, uint32_t img_bytes,
                                         const Handoff &ho, cosims_traj_out *out,
                                         unsigned long long *counters) {
   const int WG = ho.wide_lanes;
-  const int nwide = blockDim.x / WG;
+  const int nwide = min((int)(blockDim.x / WG), 15);   // named barriers 1..15
   const int wg = threadIdx.x / WG;
   if (wg >= nwide) return;           // threads beyond whole wide groups sit out
   unsigned char *base = scratch_base(smem, img_bytes) + (size_t)wg * wide_group_bytes(WG, mode_stride);

@@ -189,8 +189,9 @@ class Context:
         return ms.value
 
     def set_handoff(self, step_budget: int = 0, wide_lanes: int = 0) -> None:
-        """Mixed form: park trajectories after step_budget steps (0 default,
-        < 0 off) and finish them in wide groups of wide_lanes threads."""
+        """Park trajectories after step_budget steps (0 default, < 0 off) and
+        finish them in wide groups: wide_lanes threads in the mixed form, the
+        whole 128-thread CTA in the plain form (bitwise the same results)."""
         check(lib().cosims_ctx_set_handoff(self._h, int(step_budget), int(wide_lanes)))
 
     def get_handoff(self) -> tuple:

@@ -185,15 +185,21 @@ cosims_status cosims_ctx_set_launch(cosims_ctx *ctx, int32_t group_lanes,
 cosims_status cosims_ctx_get_launch(const cosims_ctx *ctx, int32_t *group_lanes,
                                     int32_t *block_threads);
 
-/* Long-trajectory hand-off of the mixed form.  A trajectory still running
- * after step_budget integration steps (all attempts) is parked and finished
- * by a wide group of wide_lanes threads once SMs run out of other work, so
- * the few very long trajectories no longer set the run time.  Results depend
- * only on the trajectory, group_lanes, step_budget and wide_lanes, not on
- * timing.  step_budget: 0 = default (2048), < 0 = off; wide_lanes: 0 =
- * default (128 up to 1024 atoms, else 256), else a multiple of 32 up to 512.
- * The context keeps a 200-byte record per trajectory of a call for this; calls
- * of more than 2^22 trajectories run without hand-off. */
+/* Long-trajectory hand-off.  A trajectory still running after step_budget
+ * integration steps (all attempts) is parked and finished by a wide group
+ * once its CTA runs out of other work, so the few very long trajectories no
+ * longer set the run time.
+ * Mixed form: the wide group is wide_lanes threads (0 = default: 128 up to
+ * 1024 atoms, else 256; else a multiple of 32 up to 512); results depend only
+ * on the trajectory, group_lanes, step_budget and wide_lanes, not on timing.
+ * Default step_budget 2048.
+ * Plain form: the wide group is the whole 128-thread CTA (wide_lanes 0 or
+ * 128), which evaluates a step's terms in parallel and adds them in the
+ * reference's order: results are bitwise those without hand-off, whatever
+ * the budget.  Default step_budget 256.
+ * step_budget: 0 = default, < 0 = off.  The context keeps a 200-byte record
+ * per trajectory of a call for this; calls of more than 2^22 trajectories run
+ * without hand-off. */
 cosims_status cosims_ctx_set_handoff(cosims_ctx *ctx, int64_t step_budget, int32_t wide_lanes);
 /* Current settings and, for the last run: trajectories parked, steps the
  * wide groups integrated, and the time they spent on it summed over wide

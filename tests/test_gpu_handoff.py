@@ -64,4 +64,6 @@ def test_handoff_settings_validated():
         assert cm.get_handoff()[0] == 2048       # default budget
     with engine.Context(mol, par, abi.PLAIN_F64) as cp:
         with pytest.raises(engine.CosimsError):
-            cp.set_handoff(100, 128)             # the plain form has no hand-off
+            cp.set_handoff(100, 64)              # the plain form's wide group is its CTA
+        cp.set_handoff(0, 0)
+        assert cp.get_handoff()[0] == 256        # the plain form's default budget

@@ -31,6 +31,24 @@ def test_plain_matches_reference(name):
     _check(out, d["ref_chi"], d["ref_succ"] == 1, d["ref_steps"], d["ref_de"])
 
 
+@pytest.mark.parametrize("name", CASES)
+def test_plain_handoff_is_bit_exact(name):
+    """With a step budget of 16 nearly every trajectory is parked and finished
+    by a whole CTA that adds the terms in the serial order: the results must be
+    the reference's bit for bit, as without the hand-off."""
+    mol, par, d = load(name)
+    p0, v0 = hits(d)
+    with engine.Context(mol, par, abi.PLAIN_F64) as ctx:
+        ctx.set_handoff(16, 0)
+        out = ctx.run_list(p0, v0)
+        parked = ctx.get_handoff()[2]
+        ctx.set_handoff(-1, 0)
+        off = ctx.run_list(p0, v0)
+    assert parked > len(p0) // 2
+    _check(out, d["ref_chi"], d["ref_succ"] == 1, d["ref_steps"], d["ref_de"])
+    np.testing.assert_array_equal(out, off)
+
+
 @pytest.mark.parametrize("name", ["c0_t5", "q128_t1", "q128_t4", "c1_t3"])
 def test_plain_matches_oracle_on_device_sampled_inputs(name):
     """Sampled start states from the device; same states through the oracle."""
