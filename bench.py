@@ -209,16 +209,21 @@ def profile_case(args, mol, par, stream, torch) -> None:
     from cosims_b200 import abi, engine
     prec = abi.MIXED if args.profile == "mixed" else abi.PLAIN_F64
     d_sums = torch.zeros(1024, dtype=torch.uint8, device="cuda")
+    if args.profile_max_steps:
+        par = type(par).from_buffer_copy(par)
+        par.max_steps = args.profile_max_steps
     with engine.Context(mol, par, prec) as ctx:
         if args.group_lanes and prec == abi.MIXED:
             ctx.set_launch(group_lanes=args.group_lanes)
+        if args.profile_budget:
+            ctx.set_handoff(args.profile_budget, 0)
         n = args.profile_traj
         for k in range(args.warmup + args.steps):
             ctx.run_sampled_device(SEED, k * n, n, 0, d_sums.data_ptr(), stream)
             ms = ctx.kernel_ms()
         torch.cuda.synchronize()
         print(json.dumps({"profile": args.profile, "traj": n, "launch": ctx.get_launch(),
-                          "last_kernel_ms": ms}))
+                          "handoff": ctx.get_handoff(), "last_kernel_ms": ms}))
 
 
 # ---- the batched and serving workloads (configurations 3 and 4) -------------------
@@ -603,6 +608,10 @@ def main():
                     help="small case for ncu: W + K integrals of --profile-traj trajectories "
                          "of one form only, no L2 flush buffer, no sweep")
     ap.add_argument("--profile-traj", type=int, default=20000)
+    ap.add_argument("--profile-budget", type=int, default=0,
+                    help="hand-off step budget of the profiled run (0: the default; < 0: off)")
+    ap.add_argument("--profile-max-steps", type=int, default=0,
+                    help="step cap of the profiled run's trajectories (0: the default)")
     ap.add_argument("--group-lanes", type=int, default=0)
     ap.add_argument("--workload", choices=["integral", "batched", "serving", "protein", "small"],
                     default="integral",

@@ -374,6 +374,7 @@ cosims_status launch_shape(const cosims_ctx *c, int64_t n, LaunchShape &ls) {
 // trajectories a call runs without hand-off.  Ready flags and counters are
 // cleared on the stream.
 constexpr int64_t kHandoffMaxRecords = 1 << 22;    // 800 MiB of records
+constexpr int64_t kTraceMaxBytes = int64_t(1) << 32;  // frames of one cosims_trace_list call
 
 cosims_status handoff_prepare(cosims_ctx *c, int64_t n, const LaunchShape &ls, Handoff &ho,
                               cudaStream_t s) {
@@ -409,7 +410,9 @@ cosims_status handoff_prepare(cosims_ctx *c, int64_t n, const LaunchShape &ls, H
 }
 
 cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0,
-                       const int32_t *d_hit, int64_t n, cosims_traj_out *d_out, void *stream) {
+                       const int32_t *d_hit, int64_t n, cosims_traj_out *d_out, void *stream,
+                       double *d_trace = nullptr, int32_t *d_trace_n = nullptr,
+                       int32_t trace_cap = 0) {
   LaunchShape ls;
   cosims_status st = launch_shape(c, n, ls);
   if (st != COSIMS_OK) return st;
@@ -444,8 +447,14 @@ cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0
   a.out = d_out;
   a.queue = c->d_queue;
   a.counters = c->d_counters;
-  st = handoff_prepare(c, n, ls, a.ho, s);
-  if (st != COSIMS_OK) return st;
+  if (d_trace) {                    // a traced call integrates in the one-thread loop only
+    a.trace = d_trace;
+    a.trace_n = d_trace_n;
+    a.trace_cap = trace_cap;
+  } else {
+    st = handoff_prepare(c, n, ls, a.ho, s);
+    if (st != COSIMS_OK) return st;
+  }
   if (!c->ev0) {
     e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
@@ -691,6 +700,62 @@ cosims_status cosims_run_list(cosims_ctx *c, const double *pos0, const double *v
   if (st != COSIMS_OK) return st;
   e = cudaMemcpyAsync(out, c->d_out, sizeof(cosims_traj_out) * n, cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return cuda_fail(e, "copy of results");
+  return check_error_flag(c, s);
+}
+
+cosims_status cosims_trace_list(cosims_ctx *c, const double *pos0, const double *vel0,
+                                int64_t n, int32_t max_frames, double *frames, int32_t *nframes,
+                                cosims_traj_out *out, void *stream) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (c->precision != COSIMS_PRECISION_PLAIN_F64)
+    return fail(COSIMS_ERR_UNSUPPORTED, "trajectory traces come from the plain FP64 form");
+  if (n < 0 || max_frames < 0) return fail(COSIMS_ERR_INVALID, "n and max_frames must be >= 0");
+  if (n == 0) return COSIMS_OK;
+  if (!pos0 || !vel0 || !out || !nframes || (max_frames > 0 && !frames))
+    return fail(COSIMS_ERR_INVALID, "pos0, vel0, out, nframes (and frames) are required");
+  const int64_t frame_bytes = n * (int64_t)max_frames * 6 * (int64_t)sizeof(double);
+  if (frame_bytes > (int64_t)kTraceMaxBytes)
+    return fail(COSIMS_ERR_INVALID, "n * max_frames * 48 bytes exceeds %lld",
+                (long long)kTraceMaxBytes);
+  DeviceGuard g(c->device);
+  cosims_status st = grow(&c->d_pos0, &c->list_cap, 3 * n);
+  if (st == COSIMS_OK) st = grow(&c->d_vel0, &c->vel_cap, 3 * n);
+  if (st == COSIMS_OK) st = grow(&c->d_out, &c->out_cap, n);
+  if (st != COSIMS_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  double *d_frames = nullptr;
+  int32_t *d_n = nullptr;
+  cudaError_t e = cudaMalloc((void **)&d_n, sizeof(int32_t) * (size_t)n);
+  if (e == cudaSuccess && frame_bytes > 0) e = cudaMalloc((void **)&d_frames, (size_t)frame_bytes);
+  if (e != cudaSuccess) {
+    cudaFree(d_n);
+    return fail(COSIMS_ERR_NOMEM, "trace buffers: %s", cudaGetErrorString(e));
+  }
+  e = cudaMemsetAsync(d_n, 0, sizeof(int32_t) * (size_t)n, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->d_pos0, pos0, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(c->d_vel0, vel0, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) {
+    // with max_frames 0 no frame is written; the counts buffer stands in as the
+    // (non-null) frame pointer that selects the traced kernel
+    st = run_core(c, c->d_pos0, c->d_vel0, nullptr, n, c->d_out, stream,
+                  d_frames ? d_frames : reinterpret_cast<double *>(d_n), d_n, max_frames);
+    if (st == COSIMS_OK) {
+      e = cudaMemcpyAsync(out, c->d_out, sizeof(cosims_traj_out) * n, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(nframes, d_n, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess && frame_bytes > 0)
+        e = cudaMemcpyAsync(frames, d_frames, (size_t)frame_bytes, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) st = cuda_fail(e, "trace copies");
+    }
+  } else {
+    st = cuda_fail(e, "trace inputs");
+  }
+  cudaFree(d_frames);
+  cudaFree(d_n);
+  if (st != COSIMS_OK) return st;
   return check_error_flag(c, s);
 }
 

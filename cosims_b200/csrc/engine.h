@@ -201,7 +201,14 @@ struct TrajArgs {
   cosims_traj_out *out;  // n records
   unsigned long long *queue;     // work counter (reset to 0 before launch)
   unsigned long long *counters;  // C_COUNT counters
-  Handoff ho;            // mixed form: long-trajectory hand-off (budget 0: off)
+  Handoff ho;            // long-trajectory hand-off (budget 0: off)
+  // plain form, per-step trace (cosims_trace_list): position and velocity
+  // after every integration step of trajectory t go to
+  // trace[(t * trace_cap + k) * 6 ..], k < trace_cap; trace_n[t] counts steps
+  double *trace;
+  int32_t *trace_n;
+  int32_t trace_cap;
+  int32_t pad1;
 };
 
 // ---- batched form ---------------------------------------------------------------

@@ -866,6 +866,7 @@ __device__ void exact_phase(const View &m, const TrajArgs &a, const Exact &x) {
   }
 }
 
+template <bool TRACE>
 __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
   extern __shared__ __align__(128) unsigned char smem[];
   __shared__ uint64_t bar;
@@ -966,6 +967,15 @@ __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
     step++;
     total++;
     nsteps++;
+    if (TRACE) {                       // only this thread writes trajectory t's frames
+      const int32_t k = a.trace_n[t];
+      if (k < a.trace_cap) {
+        double *f = a.trace + ((size_t)t * (size_t)a.trace_cap + (size_t)k) * 6;
+        f[0] = pos[0]; f[1] = pos[1]; f[2] = pos[2];
+        f[3] = vel[0]; f[4] = vel[1]; f[5] = vel[2];
+      }
+      a.trace_n[t] = k + 1;
+    }
     bool track = true;
     const double rold = rdot;
     rdot = dot3(pos, vel);
@@ -1001,7 +1011,8 @@ __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
     }
     // a long trajectory goes to the CTA's exact wide phase (a function of the
     // trajectory alone: its own step count; a record per trajectory exists)
-    if ((phase == P_STEP || phase == P_INIT_RETRY) && a.ho.budget > 0 && total >= a.ho.budget) {
+    if (!TRACE && (phase == P_STEP || phase == P_INIT_RETRY) && a.ho.budget > 0 &&
+        total >= a.ho.budget) {
       const unsigned long long r = atomicAdd(a.ho.reserve, 1ull);
       if (r < (unsigned long long)a.ho.cap) {
         TrajState &R = a.ho.states[r];
@@ -1025,7 +1036,7 @@ __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
   count_add(c, C_PAIR_ES, w.es);
   count_add(c, C_PAIR_POT, w.pot);
   count_add(c, C_FAR, w.far);
-  if (a.ho.budget > 0) {
+  if (!TRACE && a.ho.budget > 0) {
     __syncthreads();                    // every thread done: the CTA goes wide
     const Exact x = exact_scratch(smem, a.use_smem ? a.img.bytes : 0u, p.force_type, m.nc);
     exact_phase(m, a, x);
@@ -1042,14 +1053,20 @@ int plain_max_smem_per_block() {
   return v - 1024;   // leave room for the static barrier word
 }
 
-int plain_launch(const TrajArgs &a, int block, int grid, size_t smem, void *stream) {
+template <bool TRACE>
+static int plain_launch_t(const TrajArgs &a, int block, int grid, size_t smem, void *stream) {
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(plain::traj_plain_kernel,
+    cudaError_t e = cudaFuncSetAttribute(plain::traj_plain_kernel<TRACE>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
   }
-  plain::traj_plain_kernel<<<grid, block, smem, (cudaStream_t)stream>>>(a);
+  plain::traj_plain_kernel<TRACE><<<grid, block, smem, (cudaStream_t)stream>>>(a);
   return (int)cudaGetLastError();
+}
+
+int plain_launch(const TrajArgs &a, int block, int grid, size_t smem, void *stream) {
+  return a.trace ? plain_launch_t<true>(a, block, grid, smem, stream)
+                 : plain_launch_t<false>(a, block, grid, smem, stream);
 }
 
 }  // namespace cosims
@@ -1057,11 +1074,11 @@ int plain_launch(const TrajArgs &a, int block, int grid, size_t smem, void *stre
 namespace cosims {
 int plain_occupancy(int block, size_t smem, int *per_sm) {
   if (smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(plain::traj_plain_kernel,
+    cudaError_t e = cudaFuncSetAttribute(plain::traj_plain_kernel<false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return (int)e;
   }
-  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, plain::traj_plain_kernel,
+  return (int)cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, plain::traj_plain_kernel<false>,
                                                             block, smem);
 }
 }  // namespace cosims

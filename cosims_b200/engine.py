@@ -51,6 +51,7 @@ def lib():
                 "cosims_ctx_get_launch": (st, [V, P(C.c_int32), P(C.c_int32)]),
                 "cosims_run_list": (st, [V, V, V, C.c_int64, V, V]),
                 "cosims_run_list_device": (st, [V, V, V, C.c_int64, V, V]),
+                "cosims_trace_list": (st, [V, V, V, C.c_int64, C.c_int32, V, V, V, V]),
                 "cosims_run_sampled": (st, [V, C.c_uint64, C.c_int64, C.c_int64, C.c_int64,
                                             P(abi.CcsSums), V, V, V]),
                 "cosims_run_sampled_device": (st, [V, C.c_uint64, C.c_int64, C.c_int64,
@@ -160,6 +161,22 @@ class Context:
         check(lib().cosims_run_list(self._h, abi.vptr(pos0), abi.vptr(vel0), pos0.shape[0],
                                     abi.vptr(out), _stream_ptr(stream)))
         return out
+
+    def trace_list(self, pos0: np.ndarray, vel0: np.ndarray, max_frames: int, stream=None):
+        """Plain form: verletVel on each start state, recording position and
+        velocity after every step.  Returns (frames [n, max_frames, 6],
+        steps integrated [n], TRAJ_OUT_DTYPE records); frames[i, :min(steps[i],
+        max_frames)] are trajectory i's."""
+        pos0 = np.ascontiguousarray(pos0, dtype=np.float64).reshape(-1, 3)
+        vel0 = np.ascontiguousarray(vel0, dtype=np.float64).reshape(-1, 3)
+        n = pos0.shape[0]
+        frames = np.zeros((n, max_frames, 6))
+        steps = np.zeros(n, dtype=np.int32)
+        out = np.zeros(n, dtype=abi.TRAJ_OUT_DTYPE)
+        check(lib().cosims_trace_list(self._h, abi.vptr(pos0), abi.vptr(vel0), n, int(max_frames),
+                                      abi.vptr(frames) if max_frames else None, abi.vptr(steps),
+                                      abi.vptr(out), _stream_ptr(stream)))
+        return frames, steps, out
 
     def run_list_device(self, d_pos0: int, d_vel0: int, n: int, d_out: int, stream=None) -> None:
         check(lib().cosims_run_list_device(self._h, C.c_void_p(d_pos0), C.c_void_p(d_vel0), n,

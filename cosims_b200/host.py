@@ -81,6 +81,10 @@ def _bind():
                                           C.c_int64, P(V)]),
         "cosims_setup_create_device": (C.c_int, [P(ConfigStruct), C.c_char_p, C.c_char_p,
                                                  C.c_int32, C.c_char_p, C.c_int64, P(V)]),
+        "cosims_setup_create_structure": (C.c_int, [P(ConfigStruct), C.c_char_p, C.c_char_p,
+                                                    C.c_int32, C.c_int32, C.c_char_p,
+                                                    C.c_int64, P(V)]),
+        "cosims_molecule_file_structures": (C.c_int, [C.c_char_p, P(C.c_int32)]),
         "cosims_setup_molecule": (C.c_int, [V, P(abi.Molecule), P(abi.Params)]),
         "cosims_setup_get_info": (C.c_int, [V, P(SetupInfo)]),
         "cosims_setup_boundary": (C.c_int64, [V, V, C.c_int64]),
@@ -131,12 +135,17 @@ class Setup:
     """Per-molecule setup: the molecule and path scalars the kernels consume."""
 
     def __init__(self, cfg: Config, mol_path: str, atom_path: str | None = None,
-                 device: int | None = None):
-        """device: run the boundary ray march on this GPU (same result)."""
+                 device: int | None = None, structure: int | None = None):
+        """device: run the boundary ray march on this GPU (same result).
+        structure: coordinate set of a multi-structure file (0-based)."""
         L = _bind()
         h = C.c_void_p()
         buf = C.create_string_buffer(1 << 16)
-        if device is None:
+        if structure is not None:
+            check(L.cosims_setup_create_structure(
+                C.byref(cfg.s), mol_path.encode(), (atom_path or "").encode(), int(structure),
+                -1 if device is None else int(device), buf, len(buf), C.byref(h)))
+        elif device is None:
             check(L.cosims_setup_create(C.byref(cfg.s), mol_path.encode(),
                                         (atom_path or "").encode(), buf, len(buf), C.byref(h)))
         else:
@@ -184,6 +193,24 @@ class Setup:
 
 def setup_from_files(mol_path: str, input_path: str | None = None, atom_path: str | None = None,
                      seed: int | None = None, threads: int | None = None,
-                     device: int | None = None) -> Setup:
+                     device: int | None = None, structure: int | None = None) -> Setup:
     return Setup(Config(mol_path, input_path, seed=seed, threads=threads), mol_path, atom_path,
-                 device=device)
+                 device=device, structure=structure)
+
+
+def count_structures(mol_path: str) -> int:
+    """Coordinate sets in an MFJ or PDB file (1 for a single-structure file)."""
+    L = _bind()
+    k = C.c_int32()
+    check(L.cosims_molecule_file_structures(mol_path.encode(), C.byref(k)))
+    return k.value
+
+
+def setup_structures(mol_path: str, input_path: str | None = None,
+                     atom_path: str | None = None, seed: int | None = None,
+                     threads: int | None = None, device: int | None = None) -> list:
+    """One Setup per coordinate set of a multi-structure file, each set up as
+    a single-structure file of that set would be; feed them to engine.Batch."""
+    cfg = Config(mol_path, input_path, seed=seed, threads=threads)
+    return [Setup(cfg, mol_path, atom_path, device=device, structure=s)
+            for s in range(count_structures(mol_path))]

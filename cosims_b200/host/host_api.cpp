@@ -216,8 +216,8 @@ cosims_status cosims_config_read(cosims_config *c, const char *input_path, const
 }
 
 static cosims_status setup_create(const cosims_config *cfg, const char *mol_path,
-                                  const char *atom_path, int device, char *log_out,
-                                  int64_t log_cap, cosims_setup **out) {
+                                  const char *atom_path, int device, int structure,
+                                  char *log_out, int64_t log_cap, cosims_setup **out) {
   if (!cfg || !mol_path || !out) return fail(COSIMS_ERR_INVALID, "config, molecule and out are required");
   *out = nullptr;
   Log log;
@@ -241,8 +241,8 @@ static cosims_status setup_create(const cosims_config *cfg, const char *mol_path
   s->flags.charged = cfg->charged != 0;
   s->flags.total_charge = cfg->charge;
   bool ok;
-  if (ext == "pdb") ok = read_pdb(path, raw, log);
-  else if (ext == "mfj") ok = read_mfj(path, s->ff, raw, s->flags, log);
+  if (ext == "pdb") ok = read_pdb(path, raw, log, structure);
+  else if (ext == "mfj") ok = read_mfj(path, s->ff, raw, s->flags, log, structure);
   else {
     delete s;
     return fail(COSIMS_ERR_IO, "molecule file must end in .pdb or .mfj: %s", mol_path);
@@ -383,14 +383,44 @@ static cosims_status setup_create(const cosims_config *cfg, const char *mol_path
 cosims_status cosims_setup_create(const cosims_config *cfg, const char *mol_path,
                                   const char *atom_path, char *log_out, int64_t log_cap,
                                   cosims_setup **out) {
-  return setup_create(cfg, mol_path, atom_path, -1, log_out, log_cap, out);
+  return setup_create(cfg, mol_path, atom_path, -1, -1, log_out, log_cap, out);
 }
 
 cosims_status cosims_setup_create_device(const cosims_config *cfg, const char *mol_path,
                                          const char *atom_path, int32_t device, char *log_out,
                                          int64_t log_cap, cosims_setup **out) {
   if (device < 0) return fail(COSIMS_ERR_INVALID, "device must be >= 0");
-  return setup_create(cfg, mol_path, atom_path, device, log_out, log_cap, out);
+  return setup_create(cfg, mol_path, atom_path, device, -1, log_out, log_cap, out);
+}
+
+static bool is_pdb_path(const char *p) {
+  std::string path = p;
+  if (path.size() < 4) return false;
+  std::string ext = path.substr(path.size() - 3);
+  std::transform(ext.begin(), ext.end(), ext.begin(), ::tolower);
+  return ext == "pdb";
+}
+
+cosims_status cosims_molecule_file_structures(const char *mol_path, int32_t *count) {
+  if (!mol_path || !count) return fail(COSIMS_ERR_INVALID, "molecule path and count are required");
+  const int k = count_structures(mol_path, is_pdb_path(mol_path));
+  if (k < 0) return fail(COSIMS_ERR_IO, "cannot read molecule file %s", mol_path);
+  *count = k;
+  return COSIMS_OK;
+}
+
+cosims_status cosims_setup_create_structure(const cosims_config *cfg, const char *mol_path,
+                                            const char *atom_path, int32_t structure,
+                                            int32_t device, char *log_out, int64_t log_cap,
+                                            cosims_setup **out) {
+  if (!mol_path) return fail(COSIMS_ERR_INVALID, "molecule path is required");
+  const int k = count_structures(mol_path, is_pdb_path(mol_path));
+  if (k < 0) return fail(COSIMS_ERR_IO, "cannot read molecule file %s", mol_path);
+  if (structure < 0 || structure >= k)
+    return fail(COSIMS_ERR_INVALID, "structure %d of a file with %d", structure, k);
+  // a single-structure file is read exactly as cosims_setup_create reads it
+  return setup_create(cfg, mol_path, atom_path, device, k == 1 ? -1 : structure, log_out,
+                      log_cap, out);
 }
 
 cosims_status cosims_setup_molecule(const cosims_setup *s, cosims_molecule *m, cosims_params *p) {

@@ -83,9 +83,14 @@ struct V3 {
 
 std::vector<FFEntry> default_force_field();
 bool read_atom_file(const std::string &path, std::vector<FFEntry> &ff, Log &log);
+// Coordinate sets in a molecule file: the MFJ header's count (at least 1), or
+// the PDB file's MODEL records (1 without them).  -1 when it cannot be read.
+int count_structures(const std::string &path, bool pdb);
+// structure < 0: the reference's reader (every record is one molecule);
+// structure >= 0: coordinate set `structure` of a multi-structure file.
 bool read_mfj(const std::string &path, const std::vector<FFEntry> &ff, RawMolecule &raw,
-              MolFlags &fl, Log &log);
-bool read_pdb(const std::string &path, RawMolecule &raw, Log &log);
+              MolFlags &fl, Log &log, int structure = -1);
+bool read_pdb(const std::string &path, RawMolecule &raw, Log &log, int structure = -1);
 bool set_properties(const RawMolecule &raw, std::vector<FFEntry> &ff, const MolFlags &fl,
                     Molecule &m, double &r_disp, double &r_mp, bool dispersion_cutoff,
                     bool multipole, Log &log);

@@ -126,9 +126,37 @@ static bool all_digits(const std::string &s, bool allow_dot, bool allow_space) {
   return true;
 }
 
-// molecule2::importMFJ (molecule2.cpp:442-647)
+static bool numeric_token(const std::string &t) {
+  if (t.empty()) return false;
+  char *end = nullptr;
+  std::strtod(t.c_str(), &end);
+  return end && *end == 0;
+}
+
+int count_structures(const std::string &path, bool pdb) {
+  std::ifstream f(path.c_str());
+  if (!f) return -1;
+  std::string line;
+  if (pdb) {
+    int models = 0;
+    while (std::getline(f, line))
+      if (line.compare(0, 5, "MODEL") == 0) models++;
+    return models > 0 ? models : 1;
+  }
+  std::getline(f, line);                 // name
+  if (!std::getline(f, line)) return -1;  // number of coordinate sets
+  const int k = atoi(strip_spaces(line).c_str());
+  return k > 1 ? k : 1;
+}
+
+// molecule2::importMFJ (molecule2.cpp:442-647).  With structure >= 0 the
+// coordinate records after the header are read line by line: a line of at
+// least five tokens whose first three are numbers is a record, any other line
+// separates sets, and set s is records s*N .. s*N+N-1 (N from the header).
+// The reference reads every record as one molecule and warns that multiple
+// coordinate sets are not supported (molecule2.cpp:497-501).
 bool read_mfj(const std::string &path, const std::vector<FFEntry> &ff, RawMolecule &raw,
-              MolFlags &fl, Log &log) {
+              MolFlags &fl, Log &log, int structure) {
   std::ifstream f(path.c_str());
   if (!f) {
     log.printf("ERROR: Cannot read molecule file.\n");
@@ -142,8 +170,13 @@ bool read_mfj(const std::string &path, const std::vector<FFEntry> &ff, RawMolecu
   else
     raw.name = line;
   std::getline(f, line);
-  if (atoi(strip_spaces(line).c_str()) > 1)
+  const int sets = std::max(1, atoi(strip_spaces(line).c_str()));
+  if (sets > 1 && structure < 0)
     log.printf(" Warning: Multiple coordinate sets not yet supported.\n");
+  if (structure >= sets) {
+    log.printf(" Error: coordinate set %d requested, the file holds %d.\n", structure, sets);
+    return false;
+  }
   std::getline(f, line);
   line = strip_spaces(line);
   if (line.empty()) log.printf(" Error: Number of atoms not specified.\n");
@@ -191,7 +224,39 @@ bool read_mfj(const std::string &path, const std::vector<FFEntry> &ff, RawMolecu
   const double unitConv = unit == "au" ? 0.529177210 : 1.0;
   std::string sx, sy, sz, sm, sq;
   double total = 0.0;
-  while (f >> sx >> sy >> sz >> sm >> sq) {
+  // the records of the requested set (structure mode)
+  std::vector<std::string> recs;
+  size_t next = 0;
+  if (structure >= 0) {
+    if (sets > 1) log.printf(" Coordinate set %d of %d.\n", structure + 1, sets);
+    int seen = 0;
+    const int first = structure * header_atoms, last = first + header_atoms;
+    while (std::getline(f, line) && seen < last) {
+      std::istringstream ls(line);
+      std::string t[5];
+      int nt = 0;
+      while (nt < 5 && ls >> t[nt]) nt++;
+      if (nt < 5 || !numeric_token(t[0]) || !numeric_token(t[1]) || !numeric_token(t[2]))
+        continue;                                   // a separator line
+      if (seen >= first)
+        for (int k = 0; k < 5; k++) recs.push_back(t[k]);
+      seen++;
+    }
+    if (seen < last || header_atoms <= 0) {
+      log.printf(" Error: coordinate set %d needs records %d..%d; the file has %d.\n",
+                 structure + 1, first + 1, last, seen);
+      return false;
+    }
+  }
+  auto next_record = [&]() -> bool {
+    if (structure < 0) return (bool)(f >> sx >> sy >> sz >> sm >> sq);
+    if (next + 5 > recs.size()) return false;
+    sx = recs[next]; sy = recs[next + 1]; sz = recs[next + 2];
+    sm = recs[next + 3]; sq = recs[next + 4];
+    next += 5;
+    return true;
+  };
+  while (next_record()) {
     RawAtom a;
     a.x = atof(sx.c_str()) * scale * unitConv;
     a.y = atof(sy.c_str()) * scale * unitConv;
@@ -221,7 +286,23 @@ bool read_mfj(const std::string &path, const std::vector<FFEntry> &ff, RawMolecu
 // molecule2::importPDB (molecule2.cpp:649-768): ATOM / HETATM records; the
 // element from columns 77-78 when the line is long enough, else the first
 // letter of the atom name (columns 13-17); coordinates from fixed columns.
-bool read_pdb(const std::string &path, RawMolecule &raw, Log &log) {
+// With structure >= 0 and MODEL records in the file, only the records of the
+// structure-th MODEL (up to its ENDMDL) are read; the reference reads all.
+bool read_pdb(const std::string &path, RawMolecule &raw, Log &log, int structure) {
+  const int models = structure >= 0 ? count_structures(path, true) : 1;
+  const bool by_model = structure >= 0 && models >= 1 && [&] {
+    std::ifstream g(path.c_str());
+    std::string l;
+    while (std::getline(g, l))
+      if (l.compare(0, 5, "MODEL") == 0) return true;
+    return false;
+  }();
+  if (structure >= models) {
+    log.printf(" Error: model %d requested, the file holds %d.\n", structure + 1, models);
+    return false;
+  }
+  int model = -1;          // index of the MODEL block being read
+  bool inside = false;
   std::ifstream f(path.c_str());
   if (!f) {
     log.printf("ERROR: Cannot read molecule file.\n");
@@ -232,9 +313,17 @@ bool read_pdb(const std::string &path, RawMolecule &raw, Log &log) {
   f.getline(buf.data(), SIZE, '\n');
   while (!f.eof()) {
     const char *t = buf.data();
+    if (by_model) {
+      if (std::strncmp(t, "MODEL", 5) == 0) {
+        model++;
+        inside = model == structure;
+      } else if (std::strncmp(t, "ENDMDL", 6) == 0) {
+        inside = false;
+      }
+    }
     const bool atom = std::strncmp(t, "ATOM", 4) == 0;
     const bool het = std::strncmp(t, "HETATM", 6) == 0;
-    if (atom || het) {
+    if ((atom || het) && (!by_model || inside)) {
       char type[10];
       int nameLen = 1;
       if (std::strlen(t) >= 78) {

@@ -213,6 +213,18 @@ cosims_status cosims_ctx_get_handoff(cosims_ctx *ctx, int64_t *step_budget, int3
  * calls it.  Blocks until the results are on the host. */
 cosims_status cosims_run_list(cosims_ctx *ctx, const double *pos0, const double *vel0,
                               int64_t n, cosims_traj_out *out, void *stream);
+/* Per-step trajectory dumps, the reference's print_traj debugging keys
+ * (monteTraj::storeTraj / printTraj, monteTraj.cpp:545-586): integrate n
+ * given start states in the plain FP64 form and record the He position and
+ * velocity after every integration step (all attempts, in order) into frames
+ * (host, [n][max_frames][6]: x, y, z, vx, vy, vz).  nframes[i] receives the
+ * steps trajectory i integrated; frames holds the first min(nframes[i],
+ * max_frames).  Results are cosims_run_list's bit for bit (the trace runs
+ * without the hand-off).  Plain contexts only; n * max_frames * 48 bytes at
+ * most 4 GiB.  Blocks until the results are on the host. */
+cosims_status cosims_trace_list(cosims_ctx *ctx, const double *pos0, const double *vel0,
+                                int64_t n, int32_t max_frames, double *frames,
+                                int32_t *nframes, cosims_traj_out *out, void *stream);
 /* Same with device pointers; stream-ordered, returns without synchronising. */
 cosims_status cosims_run_list_device(cosims_ctx *ctx, const double *d_pos0,
                                      const double *d_vel0, int64_t n,

@@ -105,6 +105,25 @@ cosims_status cosims_setup_create(const cosims_config *cfg, const char *mol_path
 cosims_status cosims_setup_create_device(const cosims_config *cfg, const char *mol_path,
                                          const char *atom_path, int32_t device, char *log,
                                          int64_t log_cap, cosims_setup **out);
+/* Multi-structure molecule files (coordinate sets / conformers), for batches
+ * fed from files.  The reference reads one coordinate set per run and warns
+ * "Multiple coordinate sets not yet supported" (molecule2.cpp:497-501).
+ * MFJ: the header's second line is the number of sets K; the records after
+ * the header are read line by line, a line of at least five tokens whose first
+ * three are numbers being a record and any other line a separator, and set s
+ * is records s*N .. s*N+N-1 (N = the header's atom count).  PDB: each
+ * MODEL .. ENDMDL block is a set; a file without MODEL records is one set.
+ * cosims_molecule_file_structures returns K (1 for a single-structure file). */
+cosims_status cosims_molecule_file_structures(const char *mol_path, int32_t *count);
+/* cosims_setup_create (device < 0) or cosims_setup_create_device (device >= 0)
+ * for coordinate set `structure` (0-based).  Each set gets the whole setup of
+ * its own (rotation, boundary, ellipsoid, clusters), so set s equals the setup
+ * of a single-structure file holding only set s, bit for bit.  For a
+ * single-structure file, set 0 is read exactly as cosims_setup_create reads it. */
+cosims_status cosims_setup_create_structure(const cosims_config *cfg, const char *mol_path,
+                                            const char *atom_path, int32_t structure,
+                                            int32_t device, char *log, int64_t log_cap,
+                                            cosims_setup **out);
 /* Views of the setup's molecule and path scalars (valid while the setup
  * lives); feed them to cosims_ctx_create. */
 cosims_status cosims_setup_molecule(const cosims_setup *s, cosims_molecule *mol,

@@ -389,9 +389,9 @@ static double angle3(const double a[3], const double b[3])
  * par->max_steps (default 2^18) or when the state turns non-finite; the
  * reference has neither stop (it would loop), and no trajectory it finishes
  * comes near the cap. */
-void oracle_verlet(const cosims_molecule *mol, const cosims_params *par,
+static void verlet(const cosims_molecule *mol, const cosims_params *par,
                    const double initPos[3], const double initVel[3],
-                   cosims_traj_out *out)
+                   cosims_traj_out *out, double *frames, int32_t fcap, int32_t *nframes)
 {
     const double a = par->ell_a, b = par->ell_b, c = par->ell_c;
     const double maxRad = fmax(a, fmax(b, c));
@@ -424,6 +424,13 @@ void oracle_verlet(const cosims_molecule *mol, const cosims_params *par,
         for (int i = 0; i < 3; i++) vel[i] = vel[i] + acc[i] * dt * 0.5;
         stepCount++;
         total_steps++;
+        if (nframes) {                 /* per-step record of position and velocity */
+            if (*nframes < fcap) {
+                double *f = frames + (size_t)*nframes * 6;
+                for (int i = 0; i < 3; i++) { f[i] = pos[i]; f[3 + i] = vel[i]; }
+            }
+            (*nframes)++;
+        }
 
         int track = 1;
         rDot_old = rDot_new;
@@ -474,6 +481,20 @@ void oracle_verlet(const cosims_molecule *mol, const cosims_params *par,
     out->steps = stepCount;
     out->status = COSIMS_TRAJ_HIT | (etries << COSIMS_TRAJ_ETRIES_SHIFT) |
                   (otries << COSIMS_TRAJ_OTRIES_SHIFT);
+}
+
+void oracle_verlet(const cosims_molecule *mol, const cosims_params *par,
+                   const double initPos[3], const double initVel[3], cosims_traj_out *out)
+{
+    verlet(mol, par, initPos, initVel, out, NULL, 0, NULL);
+}
+
+void oracle_verlet_trace(const cosims_molecule *mol, const cosims_params *par,
+                         const double initPos[3], const double initVel[3],
+                         cosims_traj_out *out, double *frames, int32_t fcap, int32_t *nframes)
+{
+    *nframes = 0;
+    verlet(mol, par, initPos, initVel, out, frames, fcap, nframes);
 }
 
 /* ---- start states and accumulation ------------------------------------- */

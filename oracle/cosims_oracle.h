@@ -24,6 +24,11 @@ double oracle_potential(const cosims_molecule *mol, const cosims_params *par,
 /* diffEqSolver::verletVel (diffEqSolver.cpp:81-211) on one start state. */
 void oracle_verlet(const cosims_molecule *mol, const cosims_params *par,
                    const double pos0[3], const double vel0[3], cosims_traj_out *out);
+/* oracle_verlet that also records position and velocity after every
+ * integration step (all attempts) into frames[cap][6]; *nframes = steps. */
+void oracle_verlet_trace(const cosims_molecule *mol, const cosims_params *par,
+                         const double pos0[3], const double vel0[3], cosims_traj_out *out,
+                         double *frames, int32_t cap, int32_t *nframes);
 /* Start state geometry and ellipsoid projection of monteTraj::setUpTraj
  * (monteTraj.cpp:235-277).  Returns 1 on a hit, 0 on a miss. */
 int oracle_start_state(const cosims_params *par, const cosims_traj_in *in,

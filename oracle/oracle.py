@@ -42,6 +42,9 @@ def lib():
                                           C.c_void_p, C.c_void_p, C.c_void_p]
             L.oracle_run_inputs.argtypes = [P(abi.Molecule), P(abi.Params), C.c_int64,
                                             C.c_void_p, C.c_void_p]
+            L.oracle_verlet_trace.argtypes = [P(abi.Molecule), P(abi.Params), C.c_void_p,
+                                              C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32,
+                                              C.c_void_p]
             L.oracle_start_state.argtypes = [P(abi.Params), C.c_void_p, C.c_void_p, C.c_void_p]
             L.oracle_start_state.restype = C.c_int
             L.oracle_reduce.argtypes = [P(abi.Params), C.c_int64, C.c_void_p, C.c_int64,
@@ -76,6 +79,23 @@ def run_list(mol: abi.MoleculeArrays, par: abi.Params, pos0: np.ndarray,
     L.oracle_run_list(C.byref(m), C.byref(par), pos0.shape[0], abi.vptr(pos0),
                       abi.vptr(vel0), abi.vptr(out))
     return out
+
+
+def trace(mol: abi.MoleculeArrays, par: abi.Params, pos0: np.ndarray, vel0: np.ndarray,
+          max_frames: int):
+    """verletVel with a per-step record: (frames [n, max_frames, 6], steps [n], outs)."""
+    L, m = lib(), mol.view()
+    pos0 = np.ascontiguousarray(pos0, dtype=np.float64).reshape(-1, 3)
+    vel0 = np.ascontiguousarray(vel0, dtype=np.float64).reshape(-1, 3)
+    n = pos0.shape[0]
+    frames = np.zeros((n, max(max_frames, 1), 6))
+    steps = np.zeros(n, np.int32)
+    out = np.zeros(n, dtype=abi.TRAJ_OUT_DTYPE)
+    for i in range(n):
+        L.oracle_verlet_trace(C.byref(m), C.byref(par), abi.vptr(pos0[i]), abi.vptr(vel0[i]),
+                              abi.vptr(out[i:i + 1]), abi.vptr(frames[i]), int(max_frames),
+                              abi.vptr(steps[i:i + 1]))
+    return frames[:, :max_frames], steps, out
 
 
 def run_inputs(mol: abi.MoleculeArrays, par: abi.Params, inputs: np.ndarray) -> np.ndarray:

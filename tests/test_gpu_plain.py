@@ -83,3 +83,34 @@ def test_plain_step_cap_reports_failure():
     capped = (out["status"] & abi.TRAJ_STEPCAP) > 0
     assert capped.any()
     assert np.all(out["chi"][capped] == np.pi / 2)
+
+
+@pytest.mark.parametrize("name", ["c0_t5", "q128_t1", "c1_t3"])
+def test_trace_equals_oracle_trace(name):
+    """cosims_trace_list: the position and velocity after every step, bit for
+    bit the oracle's (all attempts), and the same results as run_list."""
+    mol, par, d = load(name)
+    p0, v0 = hits(d)
+    p0, v0 = p0[:24], v0[:24]
+    cap = 200                                   # some trajectories run past it
+    with engine.Context(mol, par, abi.PLAIN_F64) as ctx:
+        fr, steps, out = ctx.trace_list(p0, v0, cap)
+        plain = ctx.run_list(p0, v0)
+        _, steps0, out0 = ctx.trace_list(p0, v0, 0)
+    rfr, rsteps, rout = oracle.trace(mol, par, p0, v0, cap)
+    np.testing.assert_array_equal(steps, rsteps)
+    np.testing.assert_array_equal(steps0, rsteps)
+    assert (steps > cap).any() and (steps <= cap).any()
+    np.testing.assert_array_equal(fr, rfr)
+    for o in (out, out0):
+        np.testing.assert_array_equal(o["status"], plain["status"])
+        np.testing.assert_array_equal(o["chi"], plain["chi"])
+        np.testing.assert_array_equal(o["steps"], plain["steps"])
+
+
+def test_trace_needs_the_plain_form():
+    mol, par, d = load("c0_t5")
+    p0, v0 = hits(d)
+    with engine.Context(mol, par, abi.MIXED) as ctx:
+        with pytest.raises(engine.CosimsError):
+            ctx.trace_list(p0[:2], v0[:2], 10)
