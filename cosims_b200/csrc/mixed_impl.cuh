@@ -179,6 +179,77 @@ __device__ __forceinline__ void pair(const View &m, const float4 &a, const float
   }
 }
 
+// Two atom pairs at once in Blackwell's packed FP32 instructions (FADD2,
+// FMUL2, FFMA2: one issue slot for two FP32 operations): component .x is the
+// first pair, .y the second, each summed into its own half of the packed
+// accumulators (folded at the end of the evaluation).  The caller passes the
+// LJ parameters (sigma^6 and the prefactor, 0 outside the cut-off) and whether
+// the pairs add the charge field (the same for both).
+struct Acc2 {
+  float2 Fx, Fy, Fz, Ex, Ey, Ez, Pxx, Pxy, Pxz, Pyy, Pyz, Pzz, Q3;
+};
+
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+
+template <int TYPE>
+__device__ __forceinline__ void pair2(const float4 &a0, const float4 &a1, const float2 &sig6,
+                                      const float2 &eps, bool es, const float2 &hx,
+                                      const float2 &hy, const float2 &hz, const float2 &lx,
+                                      const float2 &ly, const float2 &lz, Acc2 &s) {
+  const float2 neg = f2(-1.0f, -1.0f);
+  // (h - a) + l: the FMA with -1 is the exact difference rounded once
+  const float2 dx = __fadd2_rn(__ffma2_rn(f2(a0.x, a1.x), neg, hx), lx);
+  const float2 dy = __fadd2_rn(__ffma2_rn(f2(a0.y, a1.y), neg, hy), ly);
+  const float2 dz = __fadd2_rn(__ffma2_rn(f2(a0.z, a1.z), neg, hz), lz);
+  const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+  const float2 ir = f2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+  const float2 ir2 = __fmul2_rn(ir, ir);
+  const float2 s6 = __fmul2_rn(sig6, __fmul2_rn(__fmul2_rn(ir2, ir2), ir2));
+  const float2 f = __fmul2_rn(__fmul2_rn(eps, ir2),
+                              __fmul2_rn(s6, __ffma2_rn(f2(2.0f, 2.0f), s6, neg)));
+  s.Fx = __ffma2_rn(f, dx, s.Fx);
+  s.Fy = __ffma2_rn(f, dy, s.Fy);
+  s.Fz = __ffma2_rn(f, dz, s.Fz);
+  if (Traits<TYPE>::kCharge && (Traits<TYPE>::kEsAlways || es)) {
+    const float2 q3 = __fmul2_rn(__fmul2_rn(f2(a0.w, a1.w), ir), ir2);
+    const float2 q5 = __fmul2_rn(q3, ir2);
+    s.Ex = __ffma2_rn(q3, dx, s.Ex);
+    s.Ey = __ffma2_rn(q3, dy, s.Ey);
+    s.Ez = __ffma2_rn(q3, dz, s.Ez);
+    s.Q3 = __fadd2_rn(s.Q3, q3);
+    const float2 wx = __fmul2_rn(q5, dx), wy = __fmul2_rn(q5, dy), wz = __fmul2_rn(q5, dz);
+    s.Pxx = __ffma2_rn(wx, dx, s.Pxx);
+    s.Pxy = __ffma2_rn(wx, dy, s.Pxy);
+    s.Pxz = __ffma2_rn(wx, dz, s.Pxz);
+    s.Pyy = __ffma2_rn(wy, dy, s.Pyy);
+    s.Pyz = __ffma2_rn(wy, dz, s.Pyz);
+    s.Pzz = __ffma2_rn(wz, dz, s.Pzz);
+  }
+}
+
+// LJ parameters of a slot under its cluster mode (pair's selection): the
+// band parameters of the cluster for variant 1's M_LJQ, 0 outside every cut-off.
+template <int TYPE>
+__device__ __forceinline__ float2 lj_params(const View &m, const float4 &b, uint32_t mode) {
+  if (TYPE == 1 && (mode & M_LJQ)) {
+    const ClusterF32 &C = m.cl[cluster_of(b)];
+    return f2(C.qsig6, C.qeps);
+  }
+  return f2(b.x, (TYPE == 4 || TYPE == 6 || (mode & (M_LJ | M_LJQ))) ? b.y : 0.0f);
+}
+
+// Fold the packed halves into the scalar accumulators.
+template <int TYPE>
+__device__ __forceinline__ void fold(const Acc2 &t, Acc &s) {
+  s.Fx += t.Fx.x + t.Fx.y; s.Fy += t.Fy.x + t.Fy.y; s.Fz += t.Fz.x + t.Fz.y;
+  if (Traits<TYPE>::kCharge) {
+    s.Ex += t.Ex.x + t.Ex.y; s.Ey += t.Ey.x + t.Ey.y; s.Ez += t.Ez.x + t.Ez.y;
+    s.Pxx += t.Pxx.x + t.Pxx.y; s.Pxy += t.Pxy.x + t.Pxy.y; s.Pxz += t.Pxz.x + t.Pxz.y;
+    s.Pyy += t.Pyy.x + t.Pyy.y; s.Pyz += t.Pyz.x + t.Pyz.y; s.Pzz += t.Pzz.x + t.Pzz.y;
+    s.Q3 += t.Q3.x + t.Q3.y;
+  }
+}
+
 struct WorkM { uint32_t lj, es, far; };
 
 // ---- lanes of one trajectory ------------------------------------------------------
@@ -229,14 +300,18 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
       in_mask |= (unsigned long long)((b >> gbase) & gbits) << c0;
     }
     constexpr uint32_t base_mode = TYPE == 3 ? M_ES : 0u;
+    Acc2 t = {};
+    const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
+    const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
     for (int base = 0; base < m.nslots; base += 2 * G) {
       const int k0 = base + lane, k1 = k0 + G;
       const float4 a0 = m.a4[k0], b0 = m.b4[k0], a1 = m.a4[k1], b1 = m.b4[k1];
       const uint32_t m0 = base_mode | (((in_mask >> cluster_of(b0)) & 1ull) ? (uint32_t)M_LJ : 0u);
       const uint32_t m1 = base_mode | (((in_mask >> cluster_of(b1)) & 1ull) ? (uint32_t)M_LJ : 0u);
-      pair<TYPE>(m, a0, b0, m0, hx, hy, hz, lx, ly, lz, s);
-      pair<TYPE>(m, a1, b1, m1, hx, hy, hz, lx, ly, lz, s);
+      const float2 p0 = lj_params<TYPE>(m, b0, m0), p1 = lj_params<TYPE>(m, b1, m1);
+      pair2<TYPE>(a0, a1, f2(p0.x, p1.x), f2(p0.y, p1.y), true, hx2, hy2, hz2, lx2, ly2, lz2, t);
     }
+    fold<TYPE>(t, s);
   } else if (Traits<TYPE>::kListed) {
     // pass 1: near/far decision per cluster (FP64), far-field terms; the
     // clusters that add pair terms go into the group's list (cluster << 8 |
@@ -277,17 +352,31 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     const int split = G == 32 ? 16 : G;
     const int sub = lane & (split - 1), half = G == 32 ? (lane >> 4) : 0;
     const int step = G == 32 ? 2 : 1;
+    Acc2 t = {};
+    const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
+    const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
     for (int i = half; i - half < count; i += step) {
       if (i < count) {
         const uint32_t e = list[i];
         const ClusterF32 &C = m.cl[e >> 8];
         const uint32_t mode = e & 0xffu;
-        for (int k = C.a0 + sub; k < C.a1; k += split) {
+        const bool es = (mode & M_ES) != 0;
+        int k = C.a0 + sub;
+        // two atoms of the cluster at once (not for the far-field variants,
+        // whose 22 scalar sums leave no registers for the packed ones)
+        for (; !Traits<TYPE>::kFar && k + split < C.a1; k += 2 * split) {
+          const float4 a0 = m.a4[k], b0 = m.b4[k], a1 = m.a4[k + split], b1 = m.b4[k + split];
+          const float2 p0 = lj_params<TYPE>(m, b0, mode), p1 = lj_params<TYPE>(m, b1, mode);
+          pair2<TYPE>(a0, a1, f2(p0.x, p1.x), f2(p0.y, p1.y), es, hx2, hy2, hz2, lx2, ly2, lz2,
+                      t);
+        }
+        for (; k < C.a1; k += split) {
           const float4 a = m.a4[k], b = m.b4[k];
           pair<TYPE>(m, a, b, mode, hx, hy, hz, lx, ly, lz, s);
         }
       }
     }
+    fold<TYPE>(t, s);
     ln.sync();
   } else if (Traits<TYPE>::kClusters) {
     // pass 1: near/far decision per cluster (FP64), far-field terms
@@ -320,23 +409,36 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     ln.sync();
     // pass 2: atom slots, 2G at a time (two independent pairs per lane; G <= 32
     // and slots come in multiples of 64, so both are in range)
+    Acc2 t = {};
+    const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
+    const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
     for (int base = 0; base < m.nslots; base += 2 * G) {
       const int k0 = base + lane, k1 = k0 + G;
       const float4 a0 = m.a4[k0], b0 = m.b4[k0], a1 = m.a4[k1], b1 = m.b4[k1];
       const uint32_t m0 = modes[cluster_of(b0)];
       const uint32_t m1 = modes[cluster_of(b1)];
-      pair<TYPE>(m, a0, b0, m0, hx, hy, hz, lx, ly, lz, s);
-      pair<TYPE>(m, a1, b1, m1, hx, hy, hz, lx, ly, lz, s);
+      if (Traits<TYPE>::kEsAlways || TYPE == 5 || ((m0 ^ m1) & M_ES) == 0) {
+        const float2 p0 = lj_params<TYPE>(m, b0, m0), p1 = lj_params<TYPE>(m, b1, m1);
+        pair2<TYPE>(a0, a1, f2(p0.x, p1.x), f2(p0.y, p1.y), (m0 & M_ES) != 0, hx2, hy2, hz2,
+                    lx2, ly2, lz2, t);
+      } else {
+        pair<TYPE>(m, a0, b0, m0, hx, hy, hz, lx, ly, lz, s);
+        pair<TYPE>(m, a1, b1, m1, hx, hy, hz, lx, ly, lz, s);
+      }
     }
+    fold<TYPE>(t, s);
     ln.sync();
   } else {
-    constexpr uint32_t mode = TYPE == 4 ? (M_ES | M_LJ) : M_LJ;
+    Acc2 t = {};
+    const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
+    const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
     for (int base = 0; base < m.nslots; base += 2 * G) {
       const int k0 = base + lane, k1 = k0 + G;
       const float4 a0 = m.a4[k0], b0 = m.b4[k0], a1 = m.a4[k1], b1 = m.b4[k1];
-      pair<TYPE>(m, a0, b0, mode, hx, hy, hz, lx, ly, lz, s);
-      pair<TYPE>(m, a1, b1, mode, hx, hy, hz, lx, ly, lz, s);
+      pair2<TYPE>(a0, a1, f2(b0.x, b1.x), f2(b0.y, b1.y), TYPE == 4, hx2, hy2, hz2, lx2, ly2,
+                  lz2, t);
     }
+    fold<TYPE>(t, s);
   }
   // group reduction (identical result in every lane of the group)
   constexpr int K = Traits<TYPE>::kFar ? 22 : (Traits<TYPE>::kCharge ? 13 : 3);
