@@ -252,6 +252,45 @@ __device__ __forceinline__ void fold(const Acc2 &t, Acc &s) {
 
 struct WorkM { uint32_t lj, es, far; };
 
+// Reduce-scatter of K values over a group of G lanes (G a power of two <= 32,
+// aligned in the warp) by recursive halving: at each level a lane keeps half
+// of the values it still holds and receives its partner's partial sums of
+// that half, so the group spends P/2 + P/4 + ... shuffles (P = K rounded up to
+// a power of two, P <= G) instead of log2(G) per value.  Lane l of the group
+// ends with the group sum of value idx; after the halving levels a plain
+// butterfly over the remaining lane bits makes the G/P lanes holding one index
+// agree bitwise (IEEE addition commutes).  The lanes holding value k are
+// k * (G / P) + j, j < G / P.
+template <int K>
+struct PowTwo {
+  static constexpr int P = K <= 1 ? 1 : K <= 2 ? 2 : K <= 4 ? 4 : K <= 8 ? 8 : K <= 16 ? 16 : 32;
+};
+
+template <int K>
+__device__ __forceinline__ float reduce_scatter(const float (&in)[K], int G, int lane, int &idx) {
+  constexpr int P = PowTwo<K>::P;
+  float v[P];
+#pragma unroll
+  for (int i = 0; i < P; i++) v[i] = i < K ? in[i] : 0.0f;
+  idx = 0;
+  int o = G >> 1;
+#pragma unroll
+  for (int c = P; c > 1; c >>= 1) {
+    const int half = c >> 1;
+    const bool up = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < half; i++) {
+      const float send = up ? v[i] : v[i + half];
+      const float keep = up ? v[i + half] : v[i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+    }
+    if (up) idx += half;
+    o >>= 1;
+  }
+  for (; o > 0; o >>= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], o);
+  return v[0];
+}
+
 // ---- lanes of one trajectory ------------------------------------------------------
 // A narrow group is G <= 32 lanes of one warp: shuffles reduce (bitwise the
 // same sums in every lane), __syncwarp orders the group's shared-memory state.
@@ -267,6 +306,24 @@ struct NarrowLanes {
   __device__ __forceinline__ void sum(T (&v)[K]) {
 #pragma unroll
     for (int k = 0; k < K; k++) v[k] = group_sum(v[k], G);
+  }
+  // float sums of 16- and 32-lane groups: reduce-scatter, then each lane
+  // fetches every value from a lane that holds it (P/2 + ... + K shuffles
+  // instead of K log2(G)); other widths use the butterfly
+  template <int K>
+  __device__ __forceinline__ void sum(float (&v)[K]) {
+    constexpr int P = PowTwo<K>::P;
+    if (K > 2 && P <= 16 && (G == 16 || G == 32)) {
+      int idx;
+      const float r = reduce_scatter<K>(v, G, lane, idx);
+      const int gbase = (threadIdx.x & 31) & ~(G - 1);
+      const int stride = G / P;
+#pragma unroll
+      for (int k = 0; k < K; k++) v[k] = __shfl_sync(0xffffffffu, r, gbase + k * stride);
+    } else {
+#pragma unroll
+      for (int k = 0; k < K; k++) v[k] = group_sum(v[k], G);
+    }
   }
 };
 
@@ -870,13 +927,10 @@ struct Wide {
   // sum of v over the group, the same in every thread
   template <int K>
   __device__ __forceinline__ void sum(float (&v)[K], int par) const {
-#pragma unroll
-    for (int k = 0; k < K; k++) v[k] = group_sum(v[k], 32);
+    int idx;
+    const float r = reduce_scatter<K>(v, 32, lane & 31, idx);
     float *slot = fslots + par * nwarps * kWideSlotFloats;
-    if ((lane & 31) == 0) {
-#pragma unroll
-      for (int k = 0; k < K; k++) slot[warp * kWideSlotFloats + k] = v[k];
-    }
+    if (idx < K) slot[warp * kWideSlotFloats + idx] = r;   // lanes of one index agree
     sync();
 #pragma unroll
     for (int k = 0; k < K; k++) v[k] = slot[k];
@@ -941,15 +995,45 @@ __device__ __forceinline__ void wide_force(const View &m, const DevParams &p, co
       }
     }
     wd.sync();
-#pragma unroll 4
-    for (int k = lane; k < m.nslots; k += WG) {
+    int k = lane;
+    if (!Traits<TYPE>::kFar) {
+      // slots k and k + WG in the two halves of the packed instructions
+      Acc2 t = {};
+      const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
+      const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
+#pragma unroll 2
+      for (; k + WG < m.nslots; k += 2 * WG) {
+        const float4 a0 = m.a4[k], b0 = m.b4[k], a1 = m.a4[k + WG], b1 = m.b4[k + WG];
+        const uint32_t m0 = modes[cluster_of(b0)], m1 = modes[cluster_of(b1)];
+        if (Traits<TYPE>::kEsAlways || TYPE == 5 || ((m0 ^ m1) & M_ES) == 0) {
+          const float2 p0 = lj_params<TYPE>(m, b0, m0), p1 = lj_params<TYPE>(m, b1, m1);
+          pair2<TYPE>(a0, a1, f2(p0.x, p1.x), f2(p0.y, p1.y), (m0 & M_ES) != 0, hx2, hy2, hz2,
+                      lx2, ly2, lz2, t);
+        } else {
+          pair<TYPE>(m, a0, b0, m0, hx, hy, hz, lx, ly, lz, s);
+          pair<TYPE>(m, a1, b1, m1, hx, hy, hz, lx, ly, lz, s);
+        }
+      }
+      fold<TYPE>(t, s);
+    }
+    for (; k < m.nslots; k += WG) {
       const float4 a = m.a4[k], b = m.b4[k];
       pair<TYPE>(m, a, b, (uint32_t)modes[cluster_of(b)], hx, hy, hz, lx, ly, lz, s);
     }
   } else {
     constexpr uint32_t mode = TYPE == 4 ? (M_ES | M_LJ) : M_LJ;
-#pragma unroll 4
-    for (int k = lane; k < m.nslots; k += WG) {
+    Acc2 t = {};
+    const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
+    const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
+    int k = lane;
+#pragma unroll 2
+    for (; k + WG < m.nslots; k += 2 * WG) {
+      const float4 a0 = m.a4[k], b0 = m.b4[k], a1 = m.a4[k + WG], b1 = m.b4[k + WG];
+      pair2<TYPE>(a0, a1, f2(b0.x, b1.x), f2(b0.y, b1.y), TYPE == 4, hx2, hy2, hz2, lx2, ly2,
+                  lz2, t);
+    }
+    fold<TYPE>(t, s);
+    for (; k < m.nslots; k += WG) {
       const float4 a = m.a4[k], b = m.b4[k];
       pair<TYPE>(m, a, b, mode, hx, hy, hz, lx, ly, lz, s);
     }

@@ -153,11 +153,17 @@ class Context:
         check(lib().cosims_ctx_get_launch(self._h, C.byref(g), C.byref(b)))
         return g.value, b.value
 
-    def run_list(self, pos0: np.ndarray, vel0: np.ndarray, stream=None) -> np.ndarray:
-        """verletVel on each start state; returns TRAJ_OUT_DTYPE records."""
+    def run_list(self, pos0: np.ndarray, vel0: np.ndarray, stream=None,
+                 out: np.ndarray | None = None) -> np.ndarray:
+        """verletVel on each start state; returns TRAJ_OUT_DTYPE records
+        (written into `out` when given, e.g. a pinned host array)."""
         pos0 = np.ascontiguousarray(pos0, dtype=np.float64).reshape(-1, 3)
         vel0 = np.ascontiguousarray(vel0, dtype=np.float64).reshape(-1, 3)
-        out = np.zeros(pos0.shape[0], dtype=abi.TRAJ_OUT_DTYPE)
+        if out is None:
+            out = np.zeros(pos0.shape[0], dtype=abi.TRAJ_OUT_DTYPE)
+        elif out.dtype != abi.TRAJ_OUT_DTYPE or out.shape[0] < pos0.shape[0] or \
+                not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("out must be a contiguous TRAJ_OUT_DTYPE array of n records")
         check(lib().cosims_run_list(self._h, abi.vptr(pos0), abi.vptr(vel0), pos0.shape[0],
                                     abi.vptr(out), _stream_ptr(stream)))
         return out
