@@ -210,8 +210,28 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   Builder b32;
   MolImage &i32 = h32.img;
   std::memset(&i32, 0, sizeof i32);
-  i32.off[S_ATOMS] = b32.add(a4.data(), sizeof(float4) * ns);
-  i32.off[S_LJ] = b32.add(b4.data(), sizeof(float4) * ns);
+  if (paired_layout(p->force_type)) {
+    // slots 2j and 2j+1 side by side: [np x (x,x,y,y)][np x (z,z,q,q)][np x (s,s,e,e)][np x cids]
+    const int np = ns / 2;
+    std::vector<unsigned char> pairs((size_t)np * (3 * sizeof(float4) + sizeof(uint2)));
+    float4 *pa = reinterpret_cast<float4 *>(pairs.data());
+    float4 *pb = pa + np, *pl = pb + np;
+    uint2 *pc = reinterpret_cast<uint2 *>(pl + np);
+    for (int j = 0; j < np; j++) {
+      const float4 &u = a4[2 * j], &v = a4[2 * j + 1], &s = b4[2 * j], &t = b4[2 * j + 1];
+      pa[j] = make_float4(u.x, v.x, u.y, v.y);
+      pb[j] = make_float4(u.z, v.z, u.w, v.w);
+      pl[j] = make_float4(s.x, t.x, s.y, t.y);
+      uint32_t c0, c1;
+      std::memcpy(&c0, &s.z, 4);
+      std::memcpy(&c1, &t.z, 4);
+      pc[j] = make_uint2(c0, c1);
+    }
+    i32.off[S_PAIRS] = b32.add(pairs.data(), pairs.size());
+  } else {
+    i32.off[S_ATOMS] = b32.add(a4.data(), sizeof(float4) * ns);
+    i32.off[S_LJ] = b32.add(b4.data(), sizeof(float4) * ns);
+  }
   i32.off[S_CLUSTERS] = b32.add(c32.data(), sizeof(ClusterF32) * nc);
   b32.finish();
   i32.bytes = (uint32_t)b32.buf.size();

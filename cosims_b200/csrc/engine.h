@@ -23,6 +23,12 @@
 //     of kSlotQuantum, with inert atoms (far away, q = sigma^6 = eps = 0,
 //     cluster id n_clusters, whose mode is always 0): every pair term of a pad
 //     atom is exactly zero, so the pair loop needs no bounds test.
+//     Variants 3, 4 and 6 (no far field, no cluster lists) hold the same
+//     values pair-interleaved instead, slots 2j and 2j+1 side by side, as four
+//     arrays over j: (x0, x1, y0, y1), (z0, z1, q0, q1), (sigma^6 0, sigma^6 1,
+//     24 eps/mu 0, 24 eps/mu 1) and the two cluster ids.  A lane's float4 load
+//     then yields the register pairs that Blackwell's packed FP32 instructions
+//     (FFMA2 and kin) take, with no moves to assemble them.
 #pragma once
 #include <cstdint>
 #include "cosims_cuda.h"
@@ -40,7 +46,11 @@ constexpr int kTrajStateBytes = 200;               // one trajectory's integrato
 constexpr int kGroupStateBytes = 240;              // TrajState + a group's counters (shared memory)
 constexpr int kWideSlotFloats = 24;                // per-warp reduction slot of a wide group
 
-enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_LJ, S_SLOTS, S_COUNT };
+enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_LJ, S_SLOTS, S_PAIRS, S_COUNT };
+// variants whose F32 image is pair-interleaved (S_PAIRS instead of S_ATOMS / S_LJ)
+__host__ __device__ constexpr bool paired_layout(int force_type) {
+  return force_type == 3 || force_type == 4 || force_type == 6;
+}
 
 struct AtomF64 {            // 56 bytes
   double x, y, z, q, sig6, eps24m, eps4;

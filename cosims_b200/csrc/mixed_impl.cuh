@@ -28,6 +28,11 @@ enum ModeBits : uint8_t { M_ES = 1, M_LJ = 2, M_LJQ = 4 };
 struct View {
   const float4 *a4;        // x, y, z, q
   const float4 *b4;        // sigma^6, 24 eps/mu, cluster id (integer bits), 0
+  // pair-interleaved layout (variants 3, 4, 6): slot pair j = atoms 2j, 2j+1
+  const float4 *px;        // x0, x1, y0, y1
+  const float4 *pz;        // z0, z1, q0, q1
+  const float4 *pl;        // sigma^6 0, sigma^6 1, 24 eps/mu 0, 24 eps/mu 1
+  const uint2 *pc;         // cluster ids
   const ClusterF32 *cl;
   int n, nc, nslots;        // atoms, clusters, padded atom slots
 };
@@ -41,6 +46,11 @@ __device__ __forceinline__ View make_view(const unsigned char *b, const MolImage
   View v;
   v.a4 = reinterpret_cast<const float4 *>(b + img.off[S_ATOMS]);
   v.b4 = reinterpret_cast<const float4 *>(b + img.off[S_LJ]);
+  const int np = img.n_slots / 2;
+  v.px = reinterpret_cast<const float4 *>(b + img.off[S_PAIRS]);
+  v.pz = v.px + np;
+  v.pl = v.pz + np;
+  v.pc = reinterpret_cast<const uint2 *>(v.pl + np);
   v.cl = reinterpret_cast<const ClusterF32 *>(b + img.off[S_CLUSTERS]);
   v.n = img.n_atoms;
   v.nc = img.n_clusters;
@@ -192,15 +202,16 @@ struct Acc2 {
 __device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
 
 template <int TYPE>
-__device__ __forceinline__ void pair2(const float4 &a0, const float4 &a1, const float2 &sig6,
-                                      const float2 &eps, bool es, const float2 &hx,
-                                      const float2 &hy, const float2 &hz, const float2 &lx,
-                                      const float2 &ly, const float2 &lz, Acc2 &s) {
+__device__ __forceinline__ void pair2v(const float2 &ax, const float2 &ay, const float2 &az,
+                                       const float2 &aq, const float2 &sig6, const float2 &eps,
+                                       bool es, const float2 &hx, const float2 &hy,
+                                       const float2 &hz, const float2 &lx, const float2 &ly,
+                                       const float2 &lz, Acc2 &s) {
   const float2 neg = f2(-1.0f, -1.0f);
   // (h - a) + l: the FMA with -1 is the exact difference rounded once
-  const float2 dx = __fadd2_rn(__ffma2_rn(f2(a0.x, a1.x), neg, hx), lx);
-  const float2 dy = __fadd2_rn(__ffma2_rn(f2(a0.y, a1.y), neg, hy), ly);
-  const float2 dz = __fadd2_rn(__ffma2_rn(f2(a0.z, a1.z), neg, hz), lz);
+  const float2 dx = __fadd2_rn(__ffma2_rn(ax, neg, hx), lx);
+  const float2 dy = __fadd2_rn(__ffma2_rn(ay, neg, hy), ly);
+  const float2 dz = __fadd2_rn(__ffma2_rn(az, neg, hz), lz);
   const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
   const float2 ir = f2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
   const float2 ir2 = __fmul2_rn(ir, ir);
@@ -211,7 +222,7 @@ __device__ __forceinline__ void pair2(const float4 &a0, const float4 &a1, const 
   s.Fy = __ffma2_rn(f, dy, s.Fy);
   s.Fz = __ffma2_rn(f, dz, s.Fz);
   if (Traits<TYPE>::kCharge && (Traits<TYPE>::kEsAlways || es)) {
-    const float2 q3 = __fmul2_rn(__fmul2_rn(f2(a0.w, a1.w), ir), ir2);
+    const float2 q3 = __fmul2_rn(__fmul2_rn(aq, ir), ir2);
     const float2 q5 = __fmul2_rn(q3, ir2);
     s.Ex = __ffma2_rn(q3, dx, s.Ex);
     s.Ey = __ffma2_rn(q3, dy, s.Ey);
@@ -225,6 +236,28 @@ __device__ __forceinline__ void pair2(const float4 &a0, const float4 &a1, const 
     s.Pyz = __ffma2_rn(wy, dz, s.Pyz);
     s.Pzz = __ffma2_rn(wz, dz, s.Pzz);
   }
+}
+
+// Two slots from the (x, y, z, q) records of the a4 layout.
+template <int TYPE>
+__device__ __forceinline__ void pair2(const float4 &a0, const float4 &a1, const float2 &sig6,
+                                      const float2 &eps, bool es, const float2 &hx,
+                                      const float2 &hy, const float2 &hz, const float2 &lx,
+                                      const float2 &ly, const float2 &lz, Acc2 &s) {
+  pair2v<TYPE>(f2(a0.x, a1.x), f2(a0.y, a1.y), f2(a0.z, a1.z), f2(a0.w, a1.w), sig6, eps, es,
+               hx, hy, hz, lx, ly, lz, s);
+}
+
+// Slot pair j of the pair-interleaved layout; eps holds the prefactors the
+// cut-off leaves (0 outside it).
+template <int TYPE>
+__device__ __forceinline__ void pair2j(const View &m, int j, const float2 &eps, bool es,
+                                       const float2 &hx, const float2 &hy, const float2 &hz,
+                                       const float2 &lx, const float2 &ly, const float2 &lz,
+                                       Acc2 &s) {
+  const float4 X = m.px[j], Z = m.pz[j], L = m.pl[j];
+  pair2v<TYPE>(f2(X.x, X.y), f2(X.z, X.w), f2(Z.x, Z.y), f2(Z.z, Z.w), f2(L.x, L.y), eps, es,
+               hx, hy, hz, lx, ly, lz, s);
 }
 
 // LJ parameters of a slot under its cluster mode (pair's selection): the
@@ -356,17 +389,18 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
       const unsigned b = __ballot_sync(0xffffffffu, in);
       in_mask |= (unsigned long long)((b >> gbase) & gbits) << c0;
     }
-    constexpr uint32_t base_mode = TYPE == 3 ? M_ES : 0u;
     Acc2 t = {};
     const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
     const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
-    for (int base = 0; base < m.nslots; base += 2 * G) {
-      const int k0 = base + lane, k1 = k0 + G;
-      const float4 a0 = m.a4[k0], b0 = m.b4[k0], a1 = m.a4[k1], b1 = m.b4[k1];
-      const uint32_t m0 = base_mode | (((in_mask >> cluster_of(b0)) & 1ull) ? (uint32_t)M_LJ : 0u);
-      const uint32_t m1 = base_mode | (((in_mask >> cluster_of(b1)) & 1ull) ? (uint32_t)M_LJ : 0u);
-      const float2 p0 = lj_params<TYPE>(m, b0, m0), p1 = lj_params<TYPE>(m, b1, m1);
-      pair2<TYPE>(a0, a1, f2(p0.x, p1.x), f2(p0.y, p1.y), true, hx2, hy2, hz2, lx2, ly2, lz2, t);
+    // slot pairs j = jb + lane (pair-interleaved layout; slots come in multiples
+    // of 64, so the n_slots / 2 pairs are a multiple of G)
+    for (int jb = 0; jb < (m.nslots >> 1); jb += G) {
+      const int j = jb + lane;
+      const uint2 c = m.pc[j];
+      const float2 e = f2(m.pl[j].z, m.pl[j].w);
+      const float2 eps = f2(((in_mask >> c.x) & 1ull) ? e.x : 0.0f,
+                            ((in_mask >> c.y) & 1ull) ? e.y : 0.0f);
+      pair2j<TYPE>(m, j, eps, true, hx2, hy2, hz2, lx2, ly2, lz2, t);
     }
     fold<TYPE>(t, s);
   } else if (Traits<TYPE>::kListed) {
@@ -469,18 +503,29 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     Acc2 t = {};
     const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
     const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
-    for (int base = 0; base < m.nslots; base += 2 * G) {
-      const int k0 = base + lane, k1 = k0 + G;
-      const float4 a0 = m.a4[k0], b0 = m.b4[k0], a1 = m.a4[k1], b1 = m.b4[k1];
-      const uint32_t m0 = modes[cluster_of(b0)];
-      const uint32_t m1 = modes[cluster_of(b1)];
-      if (Traits<TYPE>::kEsAlways || TYPE == 5 || ((m0 ^ m1) & M_ES) == 0) {
-        const float2 p0 = lj_params<TYPE>(m, b0, m0), p1 = lj_params<TYPE>(m, b1, m1);
-        pair2<TYPE>(a0, a1, f2(p0.x, p1.x), f2(p0.y, p1.y), (m0 & M_ES) != 0, hx2, hy2, hz2,
-                    lx2, ly2, lz2, t);
-      } else {
-        pair<TYPE>(m, a0, b0, m0, hx, hy, hz, lx, ly, lz, s);
-        pair<TYPE>(m, a1, b1, m1, hx, hy, hz, lx, ly, lz, s);
+    if (paired_layout(TYPE)) {
+      // variant 3: every slot adds the charge field, the mode only switches LJ
+      for (int jb = 0; jb < (m.nslots >> 1); jb += G) {
+        const int j = jb + lane;
+        const uint2 c = m.pc[j];
+        const float2 e = f2(m.pl[j].z, m.pl[j].w);
+        const float2 eps = f2((modes[c.x] & M_LJ) ? e.x : 0.0f, (modes[c.y] & M_LJ) ? e.y : 0.0f);
+        pair2j<TYPE>(m, j, eps, true, hx2, hy2, hz2, lx2, ly2, lz2, t);
+      }
+    } else {
+      for (int base = 0; base < m.nslots; base += 2 * G) {
+        const int k0 = base + lane, k1 = k0 + G;
+        const float4 a0 = m.a4[k0], b0 = m.b4[k0], a1 = m.a4[k1], b1 = m.b4[k1];
+        const uint32_t m0 = modes[cluster_of(b0)];
+        const uint32_t m1 = modes[cluster_of(b1)];
+        if (Traits<TYPE>::kEsAlways || TYPE == 5 || ((m0 ^ m1) & M_ES) == 0) {
+          const float2 p0 = lj_params<TYPE>(m, b0, m0), p1 = lj_params<TYPE>(m, b1, m1);
+          pair2<TYPE>(a0, a1, f2(p0.x, p1.x), f2(p0.y, p1.y), (m0 & M_ES) != 0, hx2, hy2, hz2,
+                      lx2, ly2, lz2, t);
+        } else {
+          pair<TYPE>(m, a0, b0, m0, hx, hy, hz, lx, ly, lz, s);
+          pair<TYPE>(m, a1, b1, m1, hx, hy, hz, lx, ly, lz, s);
+        }
       }
     }
     fold<TYPE>(t, s);
@@ -489,11 +534,9 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     Acc2 t = {};
     const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
     const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
-    for (int base = 0; base < m.nslots; base += 2 * G) {
-      const int k0 = base + lane, k1 = k0 + G;
-      const float4 a0 = m.a4[k0], b0 = m.b4[k0], a1 = m.a4[k1], b1 = m.b4[k1];
-      pair2<TYPE>(a0, a1, f2(b0.x, b1.x), f2(b0.y, b1.y), TYPE == 4, hx2, hy2, hz2, lx2, ly2,
-                  lz2, t);
+    for (int jb = 0; jb < (m.nslots >> 1); jb += G) {
+      const int j = jb + lane;
+      pair2j<TYPE>(m, j, f2(m.pl[j].z, m.pl[j].w), TYPE == 4, hx2, hy2, hz2, lx2, ly2, lz2, t);
     }
     fold<TYPE>(t, s);
   }
@@ -996,7 +1039,20 @@ __device__ __forceinline__ void wide_force(const View &m, const DevParams &p, co
     }
     wd.sync();
     int k = lane;
-    if (!Traits<TYPE>::kFar) {
+    if (paired_layout(TYPE)) {
+      // variant 3: slot pairs of the pair-interleaved layout, LJ by cluster mode
+      Acc2 t = {};
+      const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
+      const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
+      for (int j = lane; j < (m.nslots >> 1); j += WG) {
+        const uint2 c = m.pc[j];
+        const float2 e = f2(m.pl[j].z, m.pl[j].w);
+        const float2 eps = f2((modes[c.x] & M_LJ) ? e.x : 0.0f, (modes[c.y] & M_LJ) ? e.y : 0.0f);
+        pair2j<TYPE>(m, j, eps, true, hx2, hy2, hz2, lx2, ly2, lz2, t);
+      }
+      fold<TYPE>(t, s);
+      k = m.nslots;
+    } else if (!Traits<TYPE>::kFar) {
       // slots k and k + WG in the two halves of the packed instructions
       Acc2 t = {};
       const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
@@ -1021,22 +1077,13 @@ __device__ __forceinline__ void wide_force(const View &m, const DevParams &p, co
       pair<TYPE>(m, a, b, (uint32_t)modes[cluster_of(b)], hx, hy, hz, lx, ly, lz, s);
     }
   } else {
-    constexpr uint32_t mode = TYPE == 4 ? (M_ES | M_LJ) : M_LJ;
+    // variants 4, 6: slot pairs of the pair-interleaved layout, every pair in full
     Acc2 t = {};
     const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
     const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
-    int k = lane;
-#pragma unroll 2
-    for (; k + WG < m.nslots; k += 2 * WG) {
-      const float4 a0 = m.a4[k], b0 = m.b4[k], a1 = m.a4[k + WG], b1 = m.b4[k + WG];
-      pair2<TYPE>(a0, a1, f2(b0.x, b1.x), f2(b0.y, b1.y), TYPE == 4, hx2, hy2, hz2, lx2, ly2,
-                  lz2, t);
-    }
+    for (int j = lane; j < (m.nslots >> 1); j += WG)
+      pair2j<TYPE>(m, j, f2(m.pl[j].z, m.pl[j].w), TYPE == 4, hx2, hy2, hz2, lx2, ly2, lz2, t);
     fold<TYPE>(t, s);
-    for (; k < m.nslots; k += WG) {
-      const float4 a = m.a4[k], b = m.b4[k];
-      pair<TYPE>(m, a, b, mode, hx, hy, hz, lx, ly, lz, s);
-    }
   }
   constexpr int K = Traits<TYPE>::kFar ? 22 : (Traits<TYPE>::kCharge ? 13 : 3);
   float v[K];
