@@ -393,14 +393,25 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
     const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
     // slot pairs j = jb + lane (pair-interleaved layout; slots come in multiples
-    // of 64, so the n_slots / 2 pairs are a multiple of G)
-    for (int jb = 0; jb < (m.nslots >> 1); jb += G) {
-      const int j = jb + lane;
-      const uint2 c = m.pc[j];
-      const float2 e = f2(m.pl[j].z, m.pl[j].w);
-      const float2 eps = f2(((in_mask >> c.x) & 1ull) ? e.x : 0.0f,
-                            ((in_mask >> c.y) & 1ull) ? e.y : 0.0f);
-      pair2j<TYPE>(m, j, eps, true, hx2, hy2, hz2, lx2, ly2, lz2, t);
+    // of 64, so the n_slots / 2 pairs are a multiple of G).  When every
+    // cluster of every group in the warp is inside the cut-off (the usual case
+    // near the molecule) the prefactors are taken as stored, with no per-slot
+    // mask test; pad atoms carry a zero prefactor either way.
+    const unsigned long long all = m.nc == 64 ? ~0ull : ((1ull << m.nc) - 1ull);
+    if (ln.all(in_mask == all)) {
+      for (int jb = 0; jb < (m.nslots >> 1); jb += G) {
+        const int j = jb + lane;
+        pair2j<TYPE>(m, j, f2(m.pl[j].z, m.pl[j].w), true, hx2, hy2, hz2, lx2, ly2, lz2, t);
+      }
+    } else {
+      for (int jb = 0; jb < (m.nslots >> 1); jb += G) {
+        const int j = jb + lane;
+        const uint2 c = m.pc[j];
+        const float2 e = f2(m.pl[j].z, m.pl[j].w);
+        const float2 eps = f2(((in_mask >> c.x) & 1ull) ? e.x : 0.0f,
+                              ((in_mask >> c.y) & 1ull) ? e.y : 0.0f);
+        pair2j<TYPE>(m, j, eps, true, hx2, hy2, hz2, lx2, ly2, lz2, t);
+      }
     }
     fold<TYPE>(t, s);
   } else if (Traits<TYPE>::kListed) {
