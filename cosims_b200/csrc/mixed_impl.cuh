@@ -90,14 +90,23 @@ struct Traits {
   static constexpr bool kEsAlways = TYPE == 3 || TYPE == 4;
 };
 
+// rsqrt.approx without the denormal handling of rsqrtf(): a pair distance is
+// never below an Angstrom squared, and pad atoms sit at 1e6 Angstrom.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+  float y;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 // Far-field monopole + dipole (+ quadrupole) terms of one cluster, in FP32,
 // the reference's far block (forceAccel.cpp:258-337).
 __device__ __forceinline__ void far_terms(const View &m, int n, int order, float dx0, float dx1,
                                           float dx2, Acc &s) {
   const float xx = dx0 * dx0, yy = dx1 * dx1, zz = dx2 * dx2;
   const float r2 = xx + yy + zz;
-  const float r_2 = 1.0f / r2;
-  const float r_1 = rsqrtf(r2);
+  // far clusters lie beyond the multipole radius: r2 is large and normal
+  const float r_1 = rsqrt_ftz(r2);
+  const float r_2 = r_1 * r_1;
   const float r_3 = r_2 * r_1;
   const float r_5 = r_3 * r_2;
   const float xy = dx0 * dx1, xz = dx0 * dx2, yz = dx1 * dx2;
@@ -142,13 +151,6 @@ __device__ __forceinline__ void far_terms(const View &m, int n, int order, float
   }
 }
 
-// rsqrt.approx without the denormal handling of rsqrtf(): a pair distance is
-// never below an Angstrom squared, and pad atoms sit at 1e6 Angstrom.
-__device__ __forceinline__ float rsqrt_ftz(float x) {
-  float y;
-  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
 
 __device__ __forceinline__ uint32_t cluster_of(const float4 &b) { return __float_as_uint(b.z); }
 
@@ -161,10 +163,13 @@ __device__ __forceinline__ uint32_t cluster_of(const float4 &b) { return __float
 template <int TYPE>
 __device__ __forceinline__ void pair(const View &m, const float4 &a, const float4 &b,
                                      uint32_t mode, float hx, float hy, float hz, float lx,
-                                     float ly, float lz, Acc &s) {
+                                     float ly, float lz, Acc &s,
+                                     const ClusterF32 *own = nullptr) {
+  // own: the slot's cluster when the caller has it (its band parameters then
+  // load once per cluster rather than per pair)
   float sig6 = b.x, eps24 = b.y;
   if (TYPE == 1 && (mode & M_LJQ)) {
-    const ClusterF32 &C = m.cl[cluster_of(b)];
+    const ClusterF32 &C = own ? *own : m.cl[cluster_of(b)];
     sig6 = C.qsig6;
     eps24 = C.qeps;
   }
@@ -474,7 +479,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         }
         for (; k < C.a1; k += split) {
           const float4 a = m.a4[k], b = m.b4[k];
-          pair<TYPE>(m, a, b, mode, hx, hy, hz, lx, ly, lz, s);
+          pair<TYPE>(m, a, b, mode, hx, hy, hz, lx, ly, lz, s, &C);
         }
       }
     }
