@@ -62,3 +62,24 @@ def test_invalid_arguments_are_rejected():
     assert L.cosims_ctx_create(C.byref(view), C.byref(bad), 0, 0, C.byref(h)) == abi.ERR_INVALID
     assert b"force_type" in L.cosims_last_error()
     assert L.cosims_ctx_create(C.byref(view), C.byref(par), 7, 0, C.byref(h)) == abi.ERR_INVALID
+
+
+def test_trace_and_structure_entry_points_reject_bad_arguments(tmp_path):
+    L = engine.lib()
+    V = C.c_void_p
+    L.cosims_trace_list.argtypes = [V, V, V, C.c_int64, C.c_int32, V, V, V, V]
+    assert L.cosims_trace_list(None, None, None, 1, 10, None, None, None, None) == abi.ERR_INVALID
+    L.cosims_molecule_file_structures.argtypes = [C.c_char_p, V]
+    k = C.c_int32()
+    assert L.cosims_molecule_file_structures(None, C.byref(k)) == abi.ERR_INVALID
+    assert L.cosims_molecule_file_structures(str(tmp_path / "none.mfj").encode(),
+                                             C.byref(k)) == abi.ERR_IO
+    from cosims_b200 import synth
+    mp = synth.config0_molecule().write_mfj(str(tmp_path / "one.mfj"))
+    assert host.count_structures(mp) == 1
+    try:
+        host.setup_from_files(mp, seed=1, structure=1)
+    except engine.CosimsError as e:
+        assert e.status == abi.ERR_INVALID
+    else:
+        raise AssertionError("a structure index past the file's sets must be rejected")
