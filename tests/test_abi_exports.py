@@ -65,11 +65,8 @@ def test_invalid_arguments_are_rejected():
 
 
 def test_trace_and_structure_entry_points_reject_bad_arguments(tmp_path):
-    L = engine.lib()
-    V = C.c_void_p
-    L.cosims_trace_list.argtypes = [V, V, V, C.c_int64, C.c_int32, V, V, V, V]
+    L = host._bind()          # the library with host and device argument types bound
     assert L.cosims_trace_list(None, None, None, 1, 10, None, None, None, None) == abi.ERR_INVALID
-    L.cosims_molecule_file_structures.argtypes = [C.c_char_p, V]
     k = C.c_int32()
     assert L.cosims_molecule_file_structures(None, C.byref(k)) == abi.ERR_INVALID
     assert L.cosims_molecule_file_structures(str(tmp_path / "none.mfj").encode(),
