@@ -15,7 +15,8 @@
 //     slots of the exact wide phase, int2 {atom (force order) or -1 for a
 //     cluster's far-field event, cluster}: cluster by cluster, a far-field
 //     slot before each cluster's atoms for variants 1 and 2.
-//   F32 image (mixed form): in force order, two float4 arrays, (x, y, z, q)
+//   F32 image (mixed form), variants 1, 2 and 5: in force order, two float4
+//     arrays, (x, y, z, q)
 //     and (sigma^6, 24 eps/mu, cluster id as integer bits, 0), so lanes
 //     reading consecutive atoms hit consecutive banks; ClusterF32 records (FP64
 //     centre and squared radii, so the near/far tests stay FP64; FP32

@@ -9,9 +9,11 @@
 // tests, the energy-conservation check (exact potential, FP64) and the
 // scattering angle; the CCS sum uses 2 sin^2(chi/2) for 1 - cos(chi).
 //
-// G lanes (1..32) work on one trajectory: they split the atoms, reduce the
-// accumulators with xor-butterfly shuffles (bitwise identical in every lane),
-// and run the integrator redundantly, so the group needs no broadcast.  The
+// G lanes (1..32) work on one trajectory: they split the atoms, two pairs per
+// packed FP32 instruction, reduce the accumulators with shuffles
+// (reduce-scatter plus broadcast for 16 and 32 lanes, xor butterfly
+// otherwise; bitwise identical in every lane), and run the integrator
+// redundantly, so the group needs no further broadcast.  The
 // physics is the reference's (forceAccel.cpp:221-884), including its
 // multipoleCutoff far band that takes sigma^6/eps of atom index n
 // (forceAccel.cpp:353-355); only the arithmetic precision and the order of the
@@ -514,8 +516,8 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
       }
     }
     ln.sync();
-    // pass 2: atom slots, 2G at a time (two independent pairs per lane; G <= 32
-    // and slots come in multiples of 64, so both are in range)
+    // pass 2: atom slots, two per lane per pass (G <= 32 and slots come in
+    // multiples of 64, so both are in range)
     Acc2 t = {};
     const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
     const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
