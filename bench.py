@@ -187,6 +187,13 @@ def roofline_traffic():
     return None
 
 
+def flops_of(s, charged: bool) -> float:
+    """Algorithmic flops of a work record (pair terms by kind)."""
+    pot = FLOPS_POT_CHARGED if charged else FLOPS_POT_NEUTRAL
+    return (FLOPS_LJ * s.pair_lj + FLOPS_ES * s.pair_es + FLOPS_FAR * s.far_terms +
+            pot * s.pair_pot)
+
+
 def autotune(ctx, stream, torch, d_sums) -> int:
     """Lanes per trajectory for this molecule: the fastest over two integrals
     of other trajectories (one integral's time varies with its longest few)."""
@@ -201,6 +208,26 @@ def autotune(ctx, stream, torch, d_sums) -> int:
             best, best_ms = g, ms
     ctx.set_launch(group_lanes=best)
     return best
+
+
+def timed_integrals(ctx, first: int, k: int, stream, torch, flush):
+    """k CCS integrals of N_TRAJ trajectories through cosims_run_integrals_device
+    (one call, device-resident records), timed on the stream with CUDA events.
+    Returns (ms of the call, per-integral sums, work record)."""
+    from cosims_b200 import abi
+    sz = abi.C.sizeof(abi.CcsSums)
+    d = torch.zeros((k + 1) * sz, dtype=torch.uint8, device="cuda")
+    flush.zero_()                                   # L2 flush before the call
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    ctx.run_integrals_device(SEED, first, N_TRAJ, k, 0, d.data_ptr(), d.data_ptr() + k * sz,
+                             stream)
+    b.record(stream)
+    torch.cuda.synchronize()
+    raw = d.cpu().numpy()
+    sums = [abi.CcsSums.from_buffer_copy(raw[i * sz:(i + 1) * sz].tobytes()) for i in range(k)]
+    work = abi.CcsSums.from_buffer_copy(raw[k * sz:(k + 1) * sz].tobytes())
+    return a.elapsed_time(b), sums, work
 
 
 def profile_case(args, mol, par, stream, torch) -> None:
@@ -223,6 +250,55 @@ def profile_case(args, mol, par, stream, torch) -> None:
         torch.cuda.synchronize()
         print(json.dumps({"profile": args.profile, "traj": n, "launch": ctx.get_launch(),
                           "handoff": ctx.get_handoff(), "last_kernel_ms": ms}))
+
+
+def parity_block(local: int) -> dict:
+    """Per-trajectory parity at the configurations' list sizes, against the
+    oracle on every host core (the cpu_baseline leg: the oracle is the
+    checker here and its per-list time is reported).  For configurations 0
+    (128-atom neutral, variant 5), 1 (512-atom +2, variant 3) and 2
+    (3000-atom +10, variant 1, 12 A multipole cut-off): the first 1e4
+    ellipsoid hits of the Philox stream with seed 7 through the plain FP64 and
+    the mixed form on the GPU and through the oracle."""
+    import numpy as np
+    from cosims_b200 import abi, engine, host, synth
+    from oracle import parity, pool
+    n_list = 10_000
+    out = {"list": f"first {n_list} ellipsoid hits of the Philox stream, seed 7",
+           "bars": {"plain_frac_within_1e-6_rad": 0.99, "plain_ccs_pct": 0.1,
+                    "mixed_ccs_pct_at_1e5": 0.3}}
+    tmp = tempfile.mkdtemp(prefix="cosims_parity_")
+    for k in (0, 1, 2):
+        mp_, ip = synth.write_case(tmp, synth.config_molecule(k), synth.CONFIG_FORCE[k])
+        st = host.setup_from_files(mp_, ip, seed=7, device=local)
+        mol, par = st.mol, st.params
+        with engine.Context(mol, par, abi.PLAIN_F64, device=local) as ctx:
+            m = int(n_list * 1.4) + 64
+            _, p0, v0, hit = ctx.sample_inputs(7, 0, m)
+            sel = np.flatnonzero(hit == 1)[:n_list]
+            p0, v0 = p0[sel], v0[sel]
+            t0 = time.perf_counter()
+            plain = ctx.run_list(p0, v0)
+            plain_s = time.perf_counter() - t0
+        with engine.Context(mol, par, abi.MIXED, device=local) as ctx:
+            mixed = ctx.run_list(p0, v0)
+        ref, wall, cpu_s = pool.run_list(mol, par, p0, v0)
+        sp, sm = parity.compare(plain, ref), parity.compare(mixed, ref)
+        out[f"config{k}"] = {
+            "atoms": int(mol.n_atoms), "force_type": int(par.force_type), "n": int(len(sel)),
+            "plain": {key: sp[key] for key in (
+                "frac_within_tol", "outside_chaotic", "outside_other", "chaotic_in_list",
+                "status_differs", "steps_differ", "max_dchi", "ccs_rel_err_pct")},
+            "mixed": {key: sm[key] for key in (
+                "dchi_p50", "dchi_p90", "dchi_p99", "max_dchi", "frac_within_tol",
+                "outside_chaotic", "outside_other", "status_differs", "ccs_rel_err_pct")},
+            "oracle": {"wall_s": round(wall, 2), "cpu_s": round(cpu_s, 2),
+                       "workers": pool.host_cores(),
+                       "traj_per_s_one_core": len(sel) / cpu_s if cpu_s > 0 else None},
+            "gpu_plain_run_list_s": round(plain_s, 3),
+        }
+    shutil.rmtree(tmp, ignore_errors=True)
+    return out
 
 
 # ---- the batched and serving workloads (configurations 3 and 4) -------------------
@@ -252,31 +328,38 @@ def config3_library(n_mol: int, seed: int = 3000):
 def setup_library(mols, device: int):
     """Reference setup of each molecule (boundary ray march on the GPU).
     Force variant: the LJ cut-off (3 charged / 5 neutral) up to 2000 atoms,
-    the 12 A multipole cut-off (variant 1) above."""
+    the 12 A multipole cut-off (variant 1) above.  Returns the (molecule,
+    params) pairs, the total seconds and each molecule's seconds."""
     from cosims_b200 import host, synth
     tmp = tempfile.mkdtemp(prefix="cosims_lib_")
-    out = []
+    out, each = [], []
     t0 = time.time()
     for m in mols:
+        t1 = time.perf_counter()
         force = "multipole12" if m.n_atoms > 2000 else "cutoff"
         mp_, ip = synth.write_case(tmp, m, force)
         st = host.setup_from_files(mp_, ip, seed=SEED, device=device)
         out.append((st.mol, st.params))
+        each.append(time.perf_counter() - t1)
     shutil.rmtree(tmp, ignore_errors=True)
-    return out, time.time() - t0
+    return out, time.time() - t0, each
 
 
-def batched_workload(args, rank, world, local, dist, torch):
+def batched_block(args, local, torch, steps: int, warmup: int, library=None) -> dict:
     """Configuration 3: 256 molecules x 2e4 trajectories in one persistent
     launch (device work queue, CUDA graph, autotuned lanes per trajectory),
-    against per-molecule plain FP64 launches timed on a stratified subset."""
+    against 256 plain FP64 per-molecule launches (every molecule, timed), with
+    each molecule's CCS error of batched against plain."""
     import numpy as np
     from cosims_b200 import abi, engine
     per_mol = 20000
     t0 = time.time()
-    mols, sizes = config3_library(args.molecules)
-    gen_s = time.time() - t0
-    lib_, setup_s = setup_library(mols, local)
+    if library is None:
+        mols, sizes = config3_library(args.molecules)
+        gen_s = time.time() - t0
+        lib_, setup_s, _ = setup_library(mols, local)
+    else:
+        lib_, sizes, gen_s, setup_s, _ = library
     ms_, pars = [m for m, _ in lib_], [p for _, p in lib_]
     k = len(ms_)
     stream = torch.cuda.current_stream()
@@ -287,48 +370,39 @@ def batched_workload(args, rank, world, local, dist, torch):
     t1 = time.time()
     b.autotune()
     tune_s = time.time() - t1
-    from cosims_b200 import shard
-    first0 = shard.first_index(rank)
-    for w in range(args.warmup):
-        b.run(seeds, np.full(k, first0 + w * per_mol, np.int64), n)
+    for w in range(warmup):
+        b.run(seeds, np.full(k, w * per_mol, np.int64), n)
     clocks = ClockSampler(local)
     clocks.start()
-    if dist:
-        dist.barrier()
     torch.cuda.synchronize()
-    step_ms, kern_ms, sums_all = [], [], []
-    for s_ in range(args.steps):
+    step_ms, kern_ms, sums_all, works = [], [], [], []
+    for s_ in range(steps):
         flush.zero_()
         a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        sums = b.run(seeds, np.full(k, first0 + (args.warmup + s_) * per_mol, np.int64), n,
-                     stream)
+        sums = b.run(seeds, np.full(k, (warmup + s_) * per_mol, np.int64), n, stream)
         e.record(stream)
         torch.cuda.synchronize()
         step_ms.append(a.elapsed_time(e))
         work, kms = b.counters()
         kern_ms.append(kms)
+        works.append(work)
         sums_all.append(sums)
-    if dist:
-        dist.barrier()
     clk = clocks.stop()
-    mean_ms = shard.max_over_ranks(sum(step_ms) / len(step_ms), dist, "cuda")
+    mean_ms = sum(step_ms) / len(step_ms)
     total = int(n.sum())
-    value = world * total / (mean_ms / 1000.0)
-    flops = FLOPS_LJ * work.pair_lj + FLOPS_ES * work.pair_es + FLOPS_FAR * work.far_terms + \
-        FLOPS_POT_CHARGED * work.pair_pot
+    value = total / (mean_ms / 1000.0)
     fp32_peak, _ = engine.probe_peaks(local)
-    achieved = flops / (kern_ms[-1] / 1000.0) / 1e12
+    achieved = sum(flops_of(w, True) for w in works) / (sum(kern_ms) / 1000.0) / 1e12
 
-    # plain FP64, one launch per molecule, on every 16th molecule by size
-    order = np.argsort(sizes)
-    subset = [int(i) for i in order[::max(1, k // 16)]]
-    first_cmp = first0 + args.warmup * per_mol
+    # plain FP64 and mixed, one launch per molecule, every molecule, on the
+    # first timed step's trajectories
+    first_cmp = warmup * per_mol
     ref = sums_all[0]
-    plain_ms, errs, mixed_ms = 0.0, [], 0.0
+    plain_ms, mixed_ms, errs = 0.0, 0.0, []
     d = torch.zeros(1024, dtype=torch.uint8, device="cuda")
     sz = abi.C.sizeof(abi.CcsSums)
-    for i in subset:
+    for i in range(k):
         with engine.Context(ms_[i], pars[i], abi.PLAIN_F64, device=local) as pc:
             a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
@@ -346,78 +420,41 @@ def batched_workload(args, rank, world, local, dist, torch):
             e.record(stream)
             torch.cuda.synchronize()
             mixed_ms += a.elapsed_time(e)
-    scale = k / len(subset)
-    plain_value = total / (plain_ms * scale / 1000.0)
-    # the subset is stratified by size: scale its time to the 256 molecules
     b.close()
-    if rank == 0:
-        types = sorted({int(p.force_type) for p in pars})
-        line = {
-            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "fp32 pair forces / fp64 integration", "data": "synthetic",
-            "config": {"workload": f"batched: {k} synthetic molecules (atoms log-normal, median "
-                                   f"400, 50..5000; charge 0..+12) x {per_mol} trajectories, "
-                                   "one persistent launch per step (CUDA graph)",
-                       "molecules": k, "atoms_total": int(sizes.sum()),
-                       "atoms_median": int(np.median(sizes)), "atoms_max": int(sizes.max()),
-                       "force_types": types, "traj_per_step": total,
-                       "l2": "flushed between steps (512 MiB write)"},
-            "ccs": {"err_pct_batched_mixed_vs_plain": {"max": max(errs),
-                                                        "mean": sum(errs) / len(errs),
-                                                        "molecules": len(subset)},
-                    "bar_pct": 0.3},
-            "plain_f64_per_molecule_launches": {
-                "value": plain_value, "unit": UNIT,
-                "estimate": f"{len(subset)} molecules (every {k // len(subset)}th by size) "
-                            f"x {per_mol} trajectories, time scaled by {scale:g}"},
-            "mixed_per_molecule_launches": {"value": total / (mixed_ms * scale / 1000.0),
-                                            "unit": UNIT},
-            "batched_over_plain": value / world / plain_value,
-            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
-                         "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
-                         "kernel": "batch_mixed_kernel", "kernel_ms": kern_ms[-1]},
-            "host_s": {"generate": round(gen_s, 1), "setup": round(setup_s, 1),
-                       "autotune": round(tune_s, 1)},
-            "gpu_launches": 3 * args.steps,   # sample, trajectories, reduce (one graph)
-            "clocks": clk,
-        }
-        print(json.dumps(line))
+    plain_value = total / (plain_ms / 1000.0)
+    types = sorted({int(p.force_type) for p in pars})
+    errs_a = np.array(errs)
+    return {
+        "workload": f"batched: {k} synthetic molecules (atoms log-normal, median 400, "
+                    f"sigma_ln 0.9, 50..5000; charge 0..+12 growing as N^(2/3)) x {per_mol} "
+                    "trajectories, one persistent launch per step (CUDA graph)",
+        "value": value, "unit": UNIT, "steps": steps, "warmup": warmup, "ms_per_step": mean_ms,
+        "molecules": k, "atoms_total": int(np.sum(sizes)), "atoms_median": int(np.median(sizes)),
+        "atoms_max": int(np.max(sizes)), "force_types": types, "traj_per_step": total,
+        "plain_f64_per_molecule_launches": {
+            "value": plain_value, "unit": UNIT, "molecules_timed": k,
+            "total_ms": plain_ms},
+        "mixed_per_molecule_launches": {"value": total / (mixed_ms / 1000.0), "unit": UNIT,
+                                        "total_ms": mixed_ms},
+        "batched_over_plain": value / plain_value,
+        "batched_over_mixed_per_molecule": value / (total / (mixed_ms / 1000.0)),
+        "ccs_err_pct_vs_plain": {"max": float(errs_a.max()), "mean": float(errs_a.mean()),
+                                 "p90": float(np.percentile(errs_a, 90)),
+                                 "molecules": k, "bar_pct": 0.3},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
+                     "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                     "kernel": "batch_mixed_kernel", "kernel_ms": sum(kern_ms) / len(kern_ms)},
+        "host_s": {"generate": round(gen_s, 1), "setup": round(setup_s, 1),
+                   "autotune": round(tune_s, 1)},
+        "clocks": clk,
+    }
 
 
-def serving_workload(args, rank, world, local, dist, torch):
-    """Configuration 4: CCS requests arrive as a Poisson stream; each names a
-    molecule of the configuration-3 library and a target relative standard
-    error (0.5 %, or 0.2 % for one request in ten).  Requests are admitted as
-    slots and HBM budget free up, run in rounds through the persistent kernel
-    with everything else in flight, and retire at their target.  Latency is
-    from arrival to retirement; the molecules' host setup is done beforehand
-    and reported apart."""
-    import numpy as np
-    from cosims_b200 import abi, engine
-    if rank != 0:
-        return
-    mols, sizes = config3_library(args.molecules)
-    lib_, setup_s = setup_library(mols, local)
-    rng = np.random.Generator(np.random.PCG64(SEED))
-    n_req = int(args.rate * args.duration * 1.5) + 16
-    gaps = rng.exponential(1.0 / args.rate, size=n_req)
-    arrivals = np.cumsum(gaps)
-    arrivals = arrivals[arrivals < args.duration]
-    which = rng.integers(0, len(lib_), size=len(arrivals))
-    target = np.where(rng.random(len(arrivals)) < 0.1, 0.002, 0.005)
-    round_traj = 8192
-    srv = engine.Server(device=local, hbm_budget=16 << 30, max_jobs=128, round_traj=round_traj)
-    # warm the kernels and the tuning on a few jobs
-    for j in range(4):
-        m, p = lib_[j]
-        jid = srv.submit(m, p, 1 + j, 0.05, min_traj=round_traj, max_traj=4 * round_traj)
-        while srv.poll(jid).state == abi.JOB_RUNNING:
-            srv.step()
-        srv.release(jid)
-    clocks = ClockSampler(local)
-    clocks.start()
+def serve_stream(srv, lib_, arrivals, which, target, seed0: int, round_traj: int):
+    """Feeds requests (arrival times in s, library index, target rel. SE) to
+    the server and steps it until every request has retired.  Returns
+    (records of done requests, wall seconds, trajectories integrated)."""
+    from cosims_b200 import abi
     t0 = time.perf_counter()
     pending, live, done = 0, {}, []
     traj_done = 0
@@ -425,8 +462,8 @@ def serving_workload(args, rank, world, local, dist, torch):
         now = time.perf_counter() - t0
         while pending < len(arrivals) and arrivals[pending] <= now:
             m, p = lib_[int(which[pending])]
-            jid = srv.submit(m, p, SEED + pending, float(target[pending]), min_traj=round_traj,
-                             max_traj=400 * round_traj)
+            jid = srv.submit(m, p, seed0 + pending, float(target[pending]),
+                             min_traj=round_traj, max_traj=400 * round_traj)
             if jid is None:
                 break                                    # no room: admit later, in order
             live[jid] = pending
@@ -441,46 +478,116 @@ def serving_workload(args, rank, world, local, dist, torch):
             stt = srv.poll(jid)
             if stt.state == abi.JOB_DONE:
                 r = live.pop(jid)
-                done.append((r, t_now - arrivals[r], stt.omega, stt.rel_se, stt.sums.n,
-                             int(which[r]), float(target[r])))
+                done.append({"req": r, "latency": t_now - arrivals[r], "omega": stt.omega,
+                             "rel_se": stt.rel_se, "n": int(stt.sums.n),
+                             "mol": int(which[r]), "target": float(target[r])})
                 traj_done += stt.sums.n
                 srv.release(jid)
-    wall = time.perf_counter() - t0
+    return done, time.perf_counter() - t0, traj_done
+
+
+def serving_block(args, local, torch, library=None, duration: float | None = None) -> dict:
+    """Configuration 4: CCS requests arrive as a Poisson stream; each names a
+    molecule of the configuration-3 library and a target relative standard
+    error (0.5 %, or 0.2 % for one request in ten).  Requests are admitted as
+    slots and HBM budget free up, run in rounds with everything else in
+    flight, and retire at their target.  The offered rate is 80 % of the
+    capacity measured on a burst of requests first (the configuration's
+    50 req/s exceeds one B200's capacity for this mix).  Latency is from
+    arrival to retirement; the per-molecule host setup is reported apart and
+    as a second latency figure with each request's own setup time added."""
+    import numpy as np
+    from cosims_b200 import abi, engine
+    duration = args.duration if duration is None else duration
+    if library is None:
+        mols, sizes = config3_library(args.molecules)
+        lib_, setup_s, per_setup = setup_library(mols, local)
+    else:
+        lib_, sizes, _, setup_s, per_setup = library
+    rng = np.random.Generator(np.random.PCG64(SEED))
+    round_traj = 8192
+    srv = engine.Server(device=local, hbm_budget=16 << 30, max_jobs=128, round_traj=round_traj)
+    # warm the kernels on a few jobs
+    for j in range(4):
+        m, p = lib_[j]
+        jid = srv.submit(m, p, 1 + j, 0.05, min_traj=round_traj, max_traj=4 * round_traj)
+        while srv.poll(jid).state == abi.JOB_RUNNING:
+            srv.step()
+        srv.release(jid)
+
+    def draw(nreq):
+        which = rng.integers(0, len(lib_), size=nreq)
+        target = np.where(rng.random(nreq) < 0.1, 0.002, 0.005)
+        return which, target
+
+    # capacity: a burst of requests all present at t = 0
+    n_burst = 48
+    w_b, t_b = draw(n_burst)
+    done_b, wall_b, _ = serve_stream(srv, lib_, np.zeros(n_burst), w_b, t_b, 10 ** 6, round_traj)
+    capacity = len(done_b) / wall_b
+    rate = args.rate if args.rate > 0 else 0.8 * capacity
+    n_req = int(rate * duration * 1.5) + 16
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
+    arrivals = arrivals[arrivals < duration]
+    which, target = draw(len(arrivals))
+    clocks = ClockSampler(local)
+    clocks.start()
+    done, wall, traj_done = serve_stream(srv, lib_, arrivals, which, target, SEED, round_traj)
     clk = clocks.stop()
-    lat = np.array([d_[1] for d_ in done])
-    # CCS of a small sample against the plain FP64 form on the same trajectories
-    sample = done[:: max(1, len(done) // 3)][:3]
+    srv.close()
+    lat = np.array([d_["latency"] for d_ in done])
+    lat_setup = np.array([d_["latency"] + per_setup[d_["mol"]] for d_ in done])
+    # 5 % of the requests against the plain FP64 form on the same trajectories
+    sample = done[::20]
     errs = []
     d = torch.zeros(1024, dtype=torch.uint8, device="cuda")
     sz = abi.C.sizeof(abi.CcsSums)
-    for (r, _, om, _, ntr, mi, _) in sample:
-        m, p = lib_[mi]
+    for r in sample:
+        m, p = lib_[r["mol"]]
         with engine.Context(m, p, abi.PLAIN_F64, device=local) as pc:
-            pc.run_sampled_device(SEED + r, 0, int(ntr), 0, d.data_ptr(),
+            pc.run_sampled_device(SEED + r["req"], 0, r["n"], 0, d.data_ptr(),
                                   torch.cuda.current_stream())
             ps = abi.CcsSums.from_buffer_copy(d.cpu().numpy()[:sz].tobytes())
-        errs.append(abs(om - ps.sum / ps.n_eff) / (ps.sum / ps.n_eff) * 100.0)
-    srv.close()
-    line = {
-        "metric": METRIC, "value": traj_done / wall, "unit": UNIT, "n_gpus": 1,
-        "steps": len(done), "warmup": 4, "ms_per_step": None, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None,
-        "dtype": "fp32 pair forces / fp64 integration", "data": "synthetic",
-        "config": {"workload": f"serving: Poisson arrivals at {args.rate:g} req/s for "
-                               f"{args.duration:g} s; molecules from a {len(lib_)}-molecule "
-                               "configuration-3 library; target rel. SE 0.5 % (0.2 % for 10 %)",
-                   "round_traj": round_traj, "max_jobs": 128},
+        om = ps.sum / ps.n_eff
+        errs.append(abs(r["omega"] - om) / om * 100.0)
+    pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None
+    return {
+        "workload": f"serving: Poisson arrivals for {duration:g} s at 80 % of the measured "
+                    f"capacity; molecules from a {len(lib_)}-molecule configuration-3 library; "
+                    "target rel. SE 0.5 % (0.2 % for 10 %)",
+        "capacity_req_per_s": capacity, "offered_req_per_s": rate,
+        "configured_req_per_s": 50.0,
         "requests": {"arrived": int(len(arrivals)), "completed": len(done),
-                     "admitted": int(pending), "per_s": len(done) / wall,
-                     "wall_s": wall},
-        "latency_s": {"p50": float(np.percentile(lat, 50)) if len(lat) else None,
-                      "p99": float(np.percentile(lat, 99)) if len(lat) else None,
-                      "max": float(lat.max()) if len(lat) else None},
-        "ccs": {"err_pct_vs_plain_f64": errs, "sample": len(errs), "bar_pct": 0.3},
-        "host_setup_s_per_molecule": setup_s / len(lib_),
+                     "completed_per_s": len(done) / wall, "wall_s": wall},
+        "value": traj_done / wall, "unit": UNIT,
+        "latency_s": {"p50": pct(lat, 50), "p99": pct(lat, 99), "max": pct(lat, 100)},
+        "latency_with_setup_s": {"p50": pct(lat_setup, 50), "p99": pct(lat_setup, 99)},
+        "host_setup_s_per_molecule": {"mean": setup_s / len(lib_),
+                                      "max": float(np.max(per_setup))},
+        "ccs_err_pct_vs_plain_f64": {"max": max(errs) if errs else None,
+                                     "mean": sum(errs) / len(errs) if errs else None,
+                                     "checked": len(errs), "bar_pct": 0.3},
+        "round_traj": round_traj, "max_jobs": 128,
         "clocks": clk,
     }
-    print(json.dumps(line))
+
+
+def batched_workload(args, rank, world, local, dist, torch):
+    if rank != 0:
+        return
+    blk = batched_block(args, local, torch, args.steps, args.warmup)
+    print(json.dumps({"metric": METRIC, "n_gpus": 1, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+                      "dtype": "fp32 pair forces / fp64 integration", **blk}))
+
+
+def serving_workload(args, rank, world, local, dist, torch):
+    if rank != 0:
+        return
+    blk = serving_block(args, local, torch)
+    print(json.dumps({"metric": METRIC, "n_gpus": 1, "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "data": "synthetic",
+                      "dtype": "fp32 pair forces / fp64 integration", **blk}))
 
 
 def molecule_workload(args, rank, world, local, dist, torch):
@@ -596,13 +703,26 @@ def molecule_workload(args, rank, world, local, dist, torch):
         print(json.dumps(line))
 
 
+def library_for_extras(args, local):
+    """The configuration-3 library, generated and set up once for the batched
+    and serving keys of the default line."""
+    t0 = time.time()
+    mols, sizes = config3_library(args.molecules)
+    gen_s = time.time() - t0
+    lib_, setup_s, per = setup_library(mols, local)
+    return lib_, sizes, gen_s, setup_s, per
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the reference program's CPU timing and the oracle parity block")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched (configuration 3) and serving (configuration 4) keys")
     ap.add_argument("--profile", choices=["mixed", "plain"], default=None,
                     help="small case for ncu: W + K integrals of --profile-traj trajectories "
                          "of one form only, no L2 flush buffer, no sweep")
@@ -619,8 +739,11 @@ def main():
                          "protein: the 3000-atom ion, 1e6 trajectories, mixed form; small: the "
                          "neutral 128-atom molecule, 1e4 trajectories, plain FP64 form")
     ap.add_argument("--molecules", type=int, default=256, help="batched/serving: library size")
-    ap.add_argument("--rate", type=float, default=50.0, help="serving: requests per second")
-    ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
+    ap.add_argument("--rate", type=float, default=0.0,
+                    help="serving: requests per second (0: 80 %% of the measured capacity)")
+    ap.add_argument("--duration", type=float, default=120.0, help="serving: seconds of arrivals")
+    ap.add_argument("--plain-integrals", type=int, default=3,
+                    help="plain FP64 integrals timed beside the mixed line")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -659,148 +782,143 @@ def main():
         profile_case(args, mol, par, stream, torch)
         return
     d_sums = torch.zeros(1024, dtype=torch.uint8, device="cuda")
-    step_sums = torch.zeros((args.steps, 128), dtype=torch.uint8, device="cuda")
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     from cosims_b200 import shard
     first0 = shard.first_index(rank)          # disjoint counter range per rank
+    K, W = args.steps, args.warmup
 
     ctx = engine.Context(mol, par, abi.MIXED, device=local)
-    g = autotune(ctx, stream, torch, d_sums)
-    for w in range(args.warmup):
-        ctx.run_sampled_device(SEED, first0 + w * N_TRAJ, N_TRAJ, 0, d_sums.data_ptr(), stream)
-    torch.cuda.synchronize()
+    g = args.group_lanes or autotune(ctx, stream, torch, d_sums)
+    ctx.set_launch(group_lanes=g)
+    # warm-up: W integrals through the same call as the timed ones
+    timed_integrals(ctx, first0, W, stream, torch, flush)
 
+    # timed: K integrals of N_TRAJ in one cosims_run_integrals call (integral k
+    # is trajectories first + k N_TRAJ ...; the call overlaps one integral's
+    # long trajectories with the next integrals' work)
     clocks = ClockSampler(local)
     clocks.start()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    kern_ms = []
-    sz = abi.C.sizeof(abi.CcsSums)
-    tails, parked = [], []
-    for k in range(args.steps):
-        flush.zero_()                                   # L2 flush between steps
-        ev[k][0].record(stream)
-        ctx.run_sampled_device(SEED, first0 + (args.warmup + k) * N_TRAJ, N_TRAJ, 0,
-                               step_sums[k].data_ptr(), stream)
-        ev[k][1].record(stream)
-        kern_ms.append(ctx.kernel_ms())
-        drain, end = ctx.kernel_timeline()
-        tails.append((drain, end))
-        parked.append(ctx.get_handoff()[2])
-    torch.cuda.synchronize()
+    call_ms, sums, work = timed_integrals(ctx, first0 + W * N_TRAJ, K, stream, torch, flush)
     if dist:
         dist.barrier()
     clk = clocks.stop()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    mean_ms = shard.max_over_ranks(sum(step_ms) / len(step_ms), dist, "cuda")
+    kern_ms = ctx.kernel_ms()                 # the trajectory launch(es) of the call
+    drain, end = ctx.kernel_timeline()
+    ho = ctx.get_handoff()
+    mean_ms = shard.max_over_ranks(call_ms / K, dist, "cuda")
     value = world * N_TRAJ / (mean_ms / 1000.0)
-
-    # work counters of the timed steps -> algorithmic flops of the trajectory kernel
-    raw = step_sums.cpu().numpy()
-    sums = [abi.CcsSums.from_buffer_copy(raw[k, :sz].tobytes()) for k in range(args.steps)]
-    pot_flops = FLOPS_POT_CHARGED if par.charged else FLOPS_POT_NEUTRAL
-    flops = [FLOPS_LJ * s.pair_lj + FLOPS_ES * s.pair_es + FLOPS_FAR * s.far_terms +
-             pot_flops * s.pair_pot for s in sums]
-    kmean = sum(kern_ms) / len(kern_ms)
-    achieved = sum(flops) / len(flops) / (kmean / 1000.0) / 1e12
+    one_launch = K * N_TRAJ <= (1 << 22)
+    flops = flops_of(work, bool(par.charged))
+    achieved = flops / ((kern_ms if one_launch else call_ms) / 1000.0) / 1e12
     fp32_peak, fp64_peak = engine.probe_peaks(local)
     tr = roofline_traffic()
     traffic = None
     if tr and tr.get("bytes_per_traj"):
-        traffic = tr["bytes_per_traj"] * N_TRAJ
+        traffic = tr["bytes_per_traj"] * N_TRAJ * K
 
     # CCS of the timed integrals (merged over ranks)
     merged = shard.merge_sums(sums, dist, "cuda")
-    omega, omega_se = merged["omega"], merged["se"]
 
-    # plain FP64 form on identical inputs: throughput and the CCS error of mixed
+    # plain FP64 form on the first timed integrals (identical inputs): its
+    # throughput through the same call, and the CCS error of mixed against it
+    P = min(args.plain_integrals, K)
     plain = engine.Context(mol, par, abi.PLAIN_F64, device=local)
-    first_cmp = first0 + args.warmup * N_TRAJ
-    plain.run_sampled_device(SEED, first_cmp, 20000, 0, d_sums.data_ptr(), stream)  # warm
-    flush.zero_()
-    pe = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-    pe[0].record(stream)
-    plain.run_sampled_device(SEED, first_cmp, N_TRAJ, 0, d_sums.data_ptr(), stream)
-    pe[1].record(stream)
-    torch.cuda.synchronize()
-    plain_ms = pe[0].elapsed_time(pe[1])
-    ps = abi.CcsSums.from_buffer_copy(d_sums.cpu().numpy()[:sz].tobytes())
-    ms0 = sums[0]
-    ccs_err = abs(ms0.sum - ps.sum) / ps.sum * 100.0
+    plain.run_integrals(SEED, first0 + W * N_TRAJ, 20000, 1)           # warm
+    plain_ms, psums, pwork = timed_integrals(plain, first0 + W * N_TRAJ, P, stream, torch, flush)
+    plain_value = world * N_TRAJ / (shard.max_over_ranks(plain_ms / P, dist, "cuda") / 1000.0)
+    errs = [abs(sums[i].sum - psums[i].sum) / psums[i].sum * 100.0 for i in range(P)]
+    pooled = abs(sum(x.sum for x in sums[:P]) - sum(x.sum for x in psums)) / \
+        sum(x.sum for x in psums) * 100.0
+    plain_kern = plain.kernel_ms()
+    plain_achieved = flops_of(pwork, bool(par.charged)) / (plain_kern / 1000.0) / 1e12
 
     # end to end through the C ABI with host buffers: the start states of the
-    # same K timed integrals (their ellipsoid hits) in pinned host memory, the
-    # per-trajectory records back into pinned host memory, copies inside the
-    # timed region
+    # K timed integrals (their ellipsoid hits) in pinned host memory, through
+    # one cosims_run_list call, the per-trajectory records back into pinned
+    # host memory; copies inside the timed region
     def pinned(x):
         return torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
-    lists = []
-    for k in range(args.steps):
-        _, p0, v0, hit = ctx.sample_inputs(SEED, first0 + (args.warmup + k) * N_TRAJ, N_TRAJ)
-        lists.append((pinned(p0[hit == 1]), pinned(v0[hit == 1])))
-    n_max = max(p.shape[0] for p, _ in lists)
-    out_pinned = torch.zeros(n_max * abi.TRAJ_OUT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    p_all, v_all = [], []
+    for k in range(K):
+        _, p0, v0, hit = ctx.sample_inputs(SEED, first0 + (W + k) * N_TRAJ, N_TRAJ)
+        p_all.append(p0[hit == 1])
+        v_all.append(v0[hit == 1])
+    p_host, v_host = pinned(np.concatenate(p_all)), pinned(np.concatenate(v_all))
+    n_e2e = p_host.shape[0]
+    out_pinned = torch.zeros(n_e2e * abi.TRAJ_OUT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
     out_host = out_pinned.numpy().view(abi.TRAJ_OUT_DTYPE)
-    ctx.run_list(lists[0][0], lists[0][1], stream, out=out_host[:lists[0][0].shape[0]])
-    e2e_ms, n_list = [], []
-    for k in range(args.steps):
-        p0, v0 = lists[k]
-        flush.zero_()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        ctx.run_list(p0, v0, stream, out=out_host[:p0.shape[0]])
-        b.record(stream)
-        torch.cuda.synchronize()
-        e2e_ms.append(a.elapsed_time(b))
-        n_list.append(p0.shape[0])
-    e2e_mean = shard.max_over_ranks(sum(e2e_ms) / len(e2e_ms), dist, "cuda")
-    n_e2e = sum(n_list) / len(n_list)
-    e2e_value = world * n_e2e / (e2e_mean / 1000.0)
+    ctx.run_list(p_host[:20000], v_host[:20000], stream, out=out_host[:20000])      # warm
+    flush.zero_()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    ctx.run_list(p_host, v_host, stream, out=out_host)
+    b.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = shard.max_over_ranks(a.elapsed_time(b), dist, "cuda")
+    e2e_value = world * n_e2e / (e2e_ms / 1000.0)
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and reference_binary():
+    cpu, parity = None, None
+    extras = rank == 0 and world == 1
+    if extras and not args.no_cpu_baseline and reference_binary():
         nc = cores()
         traj = reference_sample_size(10.0, nc)
         t = run_reference(mp, traj, 1, nc)
         cpu = {"value": traj / t[0], "unit": UNIT, "cores": nc, "kind": "reference",
                "sample": f"one integral of {traj} trajectories of the same molecule and "
                          f"input (reference program, OpenMP threads = {nc})"}
+    if extras and not args.no_cpu_baseline:
+        parity = parity_block(local)
+    batched = serving = None
+    if extras and not args.no_extras:
+        library = library_for_extras(args, local)
+        batched = batched_block(args, local, torch, 5, 3, library)
+        serving = serving_block(args, local, torch, library)
 
-    ho = ctx.get_handoff()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_ms,
+            "steps": K, "warmup": W, "ms_per_step": mean_ms,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "fp32 pair forces / fp64 integration", "data": "synthetic",
-            "config": config_block(g, "flushed between steps (512 MiB write)"),
-            "ccs": {"omega_A2": omega, "se_A2": omega_se,
-                    "err_pct_mixed_vs_plain": ccs_err, "bar_pct": 0.3},
-            "plain_f64": {"value": N_TRAJ / (plain_ms / 1000.0), "ms_per_step": plain_ms},
-            "mixed_over_plain": value / world / (N_TRAJ / (plain_ms / 1000.0)),
+            "config": config_block(g, f"the timed call's per-trajectory buffers (start states, "
+                                      f"hits, work order, records, about 120 B x {K * N_TRAJ}) "
+                                      "exceed L2; also flushed before the call (512 MiB write)"),
+            "ccs": {"omega_A2": merged["omega"], "se_A2": merged["se"],
+                    "err_pct_mixed_vs_plain": {"per_integral_max": max(errs),
+                                               "pooled": pooled, "integrals": P},
+                    "bar_pct": 0.3},
+            "plain_f64": {"value": plain_value, "ms_per_step": plain_ms / P, "integrals": P,
+                          "roofline": {"bound": "fp64", "achieved": plain_achieved,
+                                       "peak": fp64_peak, "frac": plain_achieved / fp64_peak,
+                                       "kernel": "traj_plain_kernel", "kernel_ms": plain_kern}},
+            "mixed_over_plain": value / plain_value,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
-                         "kernel": "traj_mixed_kernel<3>",
-                         "kernel_ms": kmean,
+                         "kernel": f"traj_mixed_kernel<{par.force_type}>",
+                         "kernel_ms": kern_ms, "launches": 1 if one_launch else None,
                          "peak_source": "measured in this run: FP32 FMA chains "
                                         "(cosims_probe_peaks); the driver's peaks file holds "
                                         "only HBM and bf16 tensor figures",
                          "fp64_peak": fp64_peak},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(48 * n_e2e),
-                    "d2h_bytes_per_step": int(24 * n_e2e),
-                    "path": "cosims_run_list: pinned host start states of each timed "
-                            "integral's ellipsoid hits -> device -> pinned host per-trajectory "
-                            "records (misses, resolved by the sampler, are not counted)"},
-            "gpu_launches": 7 * args.steps,   # sample, 3 x work order, trajectories, 2 x reduce
+            "parity": parity,
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": int(48 * n_e2e / K),
+                    "d2h_bytes_per_step": int(24 * n_e2e / K),
+                    "path": "cosims_run_list: pinned host start states of the K timed "
+                            "integrals' ellipsoid hits -> device -> pinned host per-trajectory "
+                            "records, one call (misses, resolved by the sampler, are not "
+                            "counted)"},
+            # sampler, 3 x work order, trajectory kernel, work counters, 2 x reduce per integral
+            "gpu_launches": 6 + 2 * K,
             "clocks": clk,
-            "tail": {"queue_drained_ms": [round(a, 2) for a, _ in tails],
-                     "kernel_end_ms": [round(b, 2) for _, b in tails],
-                     "handoff": {"step_budget": ho[0], "wide_lanes": ho[1],
-                                 "parked_per_step": parked}},
+            "tail": {"queue_drained_ms": round(drain, 2), "kernel_end_ms": round(end, 2),
+                     "handoff": {"step_budget": ho[0], "wide_lanes": ho[1], "parked": ho[2]}},
+            "batched": batched,
+            "serving": serving,
         }
         print(json.dumps(line))
     ctx.close()

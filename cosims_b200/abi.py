@@ -18,6 +18,9 @@ OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_IO, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_
 PLAIN_F64 = 0
 MIXED = 1
 
+WAIT_TEST_STAGING = 0x1
+WAIT_TEST_HANDOFF = 0x2
+
 TRAJ_HIT = 0x1
 TRAJ_SUCCESS = 0x2
 TRAJ_STEPCAP = 0x4

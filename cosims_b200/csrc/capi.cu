@@ -82,9 +82,32 @@ cosims_status validate(const cosims_molecule *mol, const cosims_params *par) {
       }
     }
   }
+  // non-finite atom data would make every trajectory non-finite (the
+  // reference reads such input unchecked and integrates NaN)
+  for (int i = 0; i < mol->n_atoms; i++) {
+    if (!std::isfinite(mol->x[i]) || !std::isfinite(mol->y[i]) || !std::isfinite(mol->z[i]) ||
+        !std::isfinite(mol->charge[i]) || !std::isfinite(mol->sig6[i]) ||
+        !std::isfinite(mol->eps24m[i]) || !std::isfinite(mol->eps4[i]))
+      return fail(COSIMS_ERR_INVALID, "atom %d has a non-finite coordinate or parameter", i);
+  }
+  if (uses) {
+    for (int c = 0; c < mol->n_clusters; c++) {
+      bool fin = std::isfinite(mol->cluster_radius[c]) && std::isfinite(mol->cluster_charge[c]);
+      for (int k = 0; k < 3; k++)
+        fin = fin && std::isfinite(mol->cluster_pos[3 * c + k]) &&
+              std::isfinite(mol->cluster_dipole[3 * c + k]);
+      for (int k = 0; k < 9; k++) fin = fin && std::isfinite(mol->cluster_quad[9 * c + k]);
+      if (!fin) return fail(COSIMS_ERR_INVALID, "cluster %d has a non-finite value", c);
+    }
+  }
   if (!(par->dt > 0) || !(par->mu > 0) || !(par->ell_a > 0) || !(par->ell_b > 0) ||
       !(par->ell_c > 0))
     return fail(COSIMS_ERR_INVALID, "dt, mu and the ellipsoid axes must be positive");
+  if (!std::isfinite(par->dt) || !std::isfinite(par->mu) || !std::isfinite(par->ell_a) ||
+      !std::isfinite(par->ell_b) || !std::isfinite(par->ell_c) || !std::isfinite(par->b_max) ||
+      !std::isfinite(par->g_min) || !std::isfinite(par->g_max) ||
+      !std::isfinite(par->ccs_const) || !std::isfinite(par->dipole_scalar))
+    return fail(COSIMS_ERR_INVALID, "the path scalars must be finite");
   if (par->multipole_order < 0 || par->multipole_order > 2)
     return fail(COSIMS_ERR_INVALID, "multipole_order must be 0, 1 or 2");
   return COSIMS_OK;
@@ -426,13 +449,15 @@ cosims_status handoff_prepare(cosims_ctx *c, int64_t n, const LaunchShape &ls, H
   ho.cap = c->ho_cap;
   ho.budget = c->ho_budget;
   ho.wide_lanes = ls.wide_lanes;
+  ho.spin_limit = c->test_spin_limit ? c->test_spin_limit : kHandoffSpinLimit;
+  ho.withhold_first = (c->test_flags & COSIMS_WAIT_TEST_HANDOFF) ? 1u : 0u;
   return COSIMS_OK;
 }
 
 cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0,
                        const int32_t *d_hit, int64_t n, cosims_traj_out *d_out, void *stream,
                        double *d_trace = nullptr, int32_t *d_trace_n = nullptr,
-                       int32_t trace_cap = 0) {
+                       int32_t trace_cap = 0, bool clear_error = true) {
   LaunchShape ls;
   cosims_status st = launch_shape(c, n, ls);
   if (st != COSIMS_OK) return st;
@@ -447,7 +472,12 @@ cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0
     if (orc != 0) return cuda_fail((cudaError_t)orc, "work-order launch");
   }
   cudaError_t e = cudaMemsetAsync(c->d_queue, 0, sizeof(unsigned long long), s);
-  if (e == cudaSuccess) e = cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * C_COUNT, s);
+  // the error flags stay set across the launches of one multi-launch call
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(c->d_counters, 0, sizeof(unsigned long long) * C_ERROR, s);
+  if (e == cudaSuccess)
+    e = cudaMemsetAsync(c->d_counters + (clear_error ? C_ERROR : C_ERROR + 1), 0,
+                        sizeof(unsigned long long) * (C_COUNT - C_ERROR - (clear_error ? 0 : 1)), s);
   if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
   if (n == 0) return COSIMS_OK;
   TrajArgs a;
@@ -459,6 +489,7 @@ cosims_status run_core(cosims_ctx *c, const double *d_pos0, const double *d_vel0
   a.group_lanes = plain ? 1 : c->group_lanes;
   a.use_smem = ls.use_smem;
   a.mode_stride = ls.mode_stride;
+  a.stage_limit = (c->test_flags & COSIMS_WAIT_TEST_STAGING) ? 0u : kStageSpinLimit;
   a.pos0 = d_pos0;
   a.vel0 = d_vel0;
   a.hit = d_hit;
@@ -512,7 +543,10 @@ cosims_status check_error_flag(cosims_ctx *c, cudaStream_t s) {
                                   cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return cuda_fail(e, "trajectory run");
-  if (flag) return fail(COSIMS_ERR_TIMEOUT, "shared-memory staging wait gave up (flags %llu)", flag);
+  if (flag)
+    return fail(COSIMS_ERR_TIMEOUT, "a bounded device wait gave up:%s%s (flags %llu)",
+                (flag & 1ull) ? " shared-memory staging" : "",
+                (flag & 2ull) ? " long-trajectory hand-off record" : "", flag);
   return COSIMS_OK;
 }
 
@@ -587,6 +621,7 @@ void cosims_ctx_destroy(cosims_ctx *c) {
   cudaFree(c->d_queue);
   cudaFree(c->d_counters);
   cudaFree(c->d_sums);
+  cudaFree(c->d_sums_many);
   cudaFree(c->d_out);
   cudaFree(c->d_in);
   cudaFree(c->d_pos0);
@@ -678,6 +713,15 @@ cosims_status cosims_ctx_set_launch(cosims_ctx *c, int32_t group_lanes, int32_t 
   }
   if (c->block_threads && c->block_threads < c->group_lanes)
     return fail(COSIMS_ERR_INVALID, "block_threads smaller than group_lanes");
+  return COSIMS_OK;
+}
+
+cosims_status cosims_ctx_set_wait_test(cosims_ctx *c, uint32_t flags, uint32_t spin_limit) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (flags & ~(uint32_t)(COSIMS_WAIT_TEST_STAGING | COSIMS_WAIT_TEST_HANDOFF))
+    return fail(COSIMS_ERR_INVALID, "unknown wait-test flags 0x%x", flags);
+  c->test_flags = flags;
+  c->test_spin_limit = spin_limit;
   return COSIMS_OK;
 }
 
@@ -818,6 +862,68 @@ cosims_status cosims_run_sampled(cosims_ctx *c, uint64_t seed, int64_t first, in
     e = cudaMemcpyAsync(outs, c->d_out, sizeof(cosims_traj_out) * n, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess && inputs && n)
     e = cudaMemcpyAsync(inputs, c->d_in, sizeof(cosims_traj_in) * n, cudaMemcpyDeviceToHost, s);
+  if (e != cudaSuccess) return cuda_fail(e, "copy of results");
+  return check_error_flag(c, s);
+}
+
+cosims_status cosims_run_integrals_device(cosims_ctx *c, uint64_t seed, int64_t first,
+                                          int64_t n_per, int32_t n_integrals,
+                                          int64_t update_every, cosims_ccs_sums *d_sums,
+                                          cosims_ccs_sums *d_work, void *stream) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (n_per < 0 || first < 0 || n_integrals < 0)
+    return fail(COSIMS_ERR_INVALID, "n_per, n_integrals and first_index must be >= 0");
+  if (n_integrals > 0 && !d_sums) return fail(COSIMS_ERR_INVALID, "sums is NULL");
+  const int64_t total = n_per * (int64_t)n_integrals;
+  if (n_per > 0 && total / n_per != n_integrals) return fail(COSIMS_ERR_INVALID, "count overflow");
+  DeviceGuard g(c->device);
+  cosims_status st = sample_into(c, seed, first, total, false, stream);
+  if (st != COSIMS_OK) return st;
+  // whole integrals per launch, at most the hand-off's record count, so every
+  // trajectory runs as it would in a call of its integral alone
+  const int64_t per_launch =
+      n_per > 0 ? std::max<int64_t>(1, kHandoffMaxRecords / n_per) : (int64_t)n_integrals;
+  for (int64_t k0 = 0; k0 < n_integrals || (k0 == 0 && d_work); k0 += per_launch) {
+    const int64_t k1 = std::min<int64_t>(n_integrals, k0 + per_launch);
+    const int64_t off = k0 * n_per, m = (k1 - k0) * n_per;
+    st = run_core(c, c->d_pos0 + 3 * off, c->d_vel0 + 3 * off, c->d_hit + off, m,
+                  c->d_out + off, stream, nullptr, nullptr, 0, k0 == 0);
+    if (st != COSIMS_OK) return st;
+    if (d_work) {
+      const int rc = add_work_launch(c->d_counters, d_work, k0 == 0 ? 1 : 0, stream);
+      if (rc != 0) return cuda_fail((cudaError_t)rc, "work counters");
+    }
+    for (int64_t k = k0; k < k1; k++) {
+      const int rc = reduce_launch(c->d_out + k * n_per, n_per, c->par.ccs_const,
+                                   c->precision == COSIMS_PRECISION_MIXED ? 1 : 0, update_every,
+                                   nullptr, d_sums + k, c->d_red, c->red_cap, stream);
+      if (rc != 0) return cuda_fail((cudaError_t)rc, "reduction launch");
+    }
+    if (n_integrals == 0) break;
+  }
+  return COSIMS_OK;
+}
+
+cosims_status cosims_run_integrals(cosims_ctx *c, uint64_t seed, int64_t first, int64_t n_per,
+                                   int32_t n_integrals, int64_t update_every,
+                                   cosims_ccs_sums *sums, cosims_ccs_sums *work, void *stream) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (n_integrals > 0 && !sums) return fail(COSIMS_ERR_INVALID, "sums is NULL");
+  if (n_integrals < 0) return fail(COSIMS_ERR_INVALID, "n_integrals must be >= 0");
+  DeviceGuard g(c->device);
+  cosims_status st = grow(&c->d_sums_many, &c->sums_cap, (int64_t)n_integrals + 1);
+  if (st != COSIMS_OK) return st;
+  cosims_ccs_sums *d_work = c->d_sums_many + n_integrals;
+  st = cosims_run_integrals_device(c, seed, first, n_per, n_integrals, update_every,
+                                   c->d_sums_many, d_work, stream);
+  if (st != COSIMS_OK) return st;
+  cudaStream_t s = (cudaStream_t)stream;
+  cudaError_t e = cudaSuccess;
+  if (n_integrals > 0)
+    e = cudaMemcpyAsync(sums, c->d_sums_many, sizeof(cosims_ccs_sums) * (size_t)n_integrals,
+                        cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess && work)
+    e = cudaMemcpyAsync(work, d_work, sizeof(cosims_ccs_sums), cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return cuda_fail(e, "copy of results");
   return check_error_flag(c, s);
 }

@@ -70,6 +70,8 @@ struct cosims_ctx {
   unsigned char *d_img64 = nullptr, *d_img32 = nullptr;
   unsigned long long *d_queue = nullptr, *d_counters = nullptr;
   cosims_ccs_sums *d_sums = nullptr;
+  cosims_ccs_sums *d_sums_many = nullptr;              // cosims_run_integrals: records + work
+  int64_t sums_cap = 0;
   cosims_traj_out *d_out = nullptr;
   int64_t out_cap = 0;
   cosims_traj_in *d_in = nullptr;
@@ -92,6 +94,9 @@ struct cosims_ctx {
   int64_t ho_cap = 0;
   unsigned long long *d_ho_ctrl = nullptr;             // reserve, taken
   int64_t ho_last_parked = 0;
+  // tests of the error path (cosims_ctx_set_wait_test)
+  uint32_t test_flags = 0;
+  uint32_t test_spin_limit = 0;
   cosims::LaunchShape last_shape{};
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;   // around the last trajectory kernel
   bool timed = false;

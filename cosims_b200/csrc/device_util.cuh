@@ -21,7 +21,6 @@ namespace cosims {
 // that never lands cannot hang the GPU.
 
 constexpr uint32_t kBulkChunk = 32768;        // bytes per bulk copy
-constexpr uint32_t kStageSpinLimit = 1u << 22;
 constexpr long long kDefaultMaxSteps = 1ll << 18;   // far above any physical trajectory
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -67,11 +66,15 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
 // Stage `bytes` (multiple of 16, both addresses 16-byte aligned, at most
 // 2^20 - 1 bytes: the mbarrier transaction-count range) from global to shared
 // memory.  Call from all threads of the CTA.  Returns false, in every thread,
-// when a bounded wait gave up (the caller flags an error and returns).
+// when the wait gave up after `limit` polls (the caller flags an error and
+// returns); before it returns, every thread waits again, at most
+// kStageSpinLimit polls, for the copies still in flight into this CTA's shared
+// memory, so the CTA does not leave while they land.
 // `init`: the first staging through this barrier (initialises it); later
 // stagings pass init = false and the parity of their phase (0, 1, 0, ...).
 __device__ __forceinline__ bool stage_to_smem(void *dst, const void *src, uint32_t bytes,
-                                              uint64_t *bar, uint32_t parity, bool init) {
+                                              uint64_t *bar, uint32_t parity, bool init,
+                                              uint32_t limit = kStageSpinLimit) {
   if (threadIdx.x == 0 && init) {
     mbar_init(bar, 1);
     fence_barrier_init();
@@ -89,11 +92,16 @@ __device__ __forceinline__ bool stage_to_smem(void *dst, const void *src, uint32
     }
   }
   bool done = false;
-  for (uint32_t spin = 0; spin < kStageSpinLimit; ++spin) {
+  for (uint32_t spin = 0; spin < limit; ++spin) {
     if (mbar_try_wait(bar, parity)) { done = true; break; }
   }
   // one decision for the whole CTA, so no thread leaves while others go on
-  return __syncthreads_and(done ? 1 : 0) != 0;
+  const bool ok = __syncthreads_and(done ? 1 : 0) != 0;
+  if (!ok) {
+    for (uint32_t spin = 0; !done && spin < kStageSpinLimit; ++spin) done = mbar_try_wait(bar, parity);
+    __syncthreads();
+  }
+  return ok;
 }
 
 // ---- Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11) ----------------------

@@ -151,8 +151,12 @@ struct Handoff {
   int64_t cap;
   int64_t budget;                  // steps before a hand-off; 0 = never
   int32_t wide_lanes;              // threads of a wide group (multiple of 32)
-  int32_t pad;
+  uint32_t spin_limit;             // polls of a wide group's wait for a record's flag
+  uint32_t withhold_first;         // test of the error path: record 0 is never published
+  uint32_t pad;
 };
+constexpr uint32_t kHandoffSpinLimit = 1u << 22;   // polls of a hand-off record's flag
+constexpr uint32_t kStageSpinLimit = 1u << 22;     // polls of a shared-memory staging wait
 
 // Shared-memory bytes of one wide group: cluster modes for two steps, then
 // per-warp reduction slots for two steps (2 x warps x 24 floats, 2 x warps x
@@ -203,7 +207,7 @@ struct TrajArgs {
   int32_t group_lanes;   // lanes per trajectory (power of two, <= 32)
   int32_t use_smem;      // image staged in shared memory (else read from global)
   int32_t mode_stride;   // bytes of per-group cluster-mode scratch in shared memory
-  int32_t pad0;
+  uint32_t stage_limit;  // polls of the shared-memory staging wait
   const double *pos0;    // 3n start positions
   const double *vel0;    // 3n start velocities
   const int32_t *hit;    // n ellipsoid hits (NULL: every start state is a hit)
@@ -286,5 +290,8 @@ int reduce_launch(const cosims_traj_out *recs, int64_t n, double ccs_const,
                   cosims_ccs_sums *d_sums, double *scratch, int64_t scratch_len,
                   void *stream);
 int64_t reduce_scratch_len(int64_t n);
+// Adds a launch's work counters into d_work (zero_first: clear it first).
+int add_work_launch(const unsigned long long *counters, cosims_ccs_sums *d_work, int zero_first,
+                    void *stream);
 
 }  // namespace cosims

@@ -693,8 +693,6 @@ __device__ __forceinline__ void traj_begin(TrajState &S, long long t, const doub
   S.phase = P_INIT_FIRST;
 }
 
-constexpr uint32_t kHandoffSpinLimit = 1u << 22;
-
 // Where a group's trajectories come from.  Narrow groups draw queue slots
 // 0..n-1 (slot k integrates trajectory order[k]; a trajectory with hit[t] == 0
 // is an ellipsoid miss, chi = 0) and may park long ones; wide groups finish
@@ -765,7 +763,7 @@ __device__ __forceinline__ bool park_to(const Handoff &ho, NarrowLanes &ln, Grou
   for (int k = ln.lane; k < kTrajStateBytes / 8; k += ln.G) g[k] = s[k];
   __threadfence();
   ln.sync();
-  if (ln.lane == 0) atomicExch(ho.ready + r, 1u);
+  if (ln.lane == 0 && !(ho.withhold_first && r == 0)) atomicExch(ho.ready + r, 1u);
   return true;
 }
 __device__ __forceinline__ bool park(const MainSource &src, NarrowLanes &ln, GroupState &GS) {
@@ -1174,7 +1172,7 @@ __device__ __forceinline__ long long wide_take(const Wide &wd, const Handoff &ho
     if (got >= 0) {
       // the parking group reserved the record before writing it: wait for its flag
       bool ok = false;
-      for (uint32_t spin = 0; spin < kHandoffSpinLimit; ++spin) {
+      for (uint32_t spin = 0; spin < ho.spin_limit; ++spin) {
         if (atomicAdd(ho.ready + got, 0u) != 0u) { ok = true; break; }
       }
       if (!ok) {
@@ -1377,7 +1375,7 @@ __global__ void __launch_bounds__(KernelShape<TYPE>::kMaxThreads, COSIMS_MIXED_M
   __shared__ uint64_t bar;
   const unsigned char *base = a.img.gbase;
   if (SMEM) {
-    if (!stage_to_smem(smem, a.img.gbase, a.img.bytes, &bar, 0, true)) {
+    if (!stage_to_smem(smem, a.img.gbase, a.img.bytes, &bar, 0, true, a.stage_limit)) {
       if (threadIdx.x == 0) atomicOr(a.counters + C_ERROR, 1ull);
       return;
     }

@@ -136,6 +136,7 @@ extern "C" cosims_status cosims_run_list_noalloc(const cosims_molecule *mol,
   a.group_lanes = G;
   a.use_smem = ls.use_smem;
   a.mode_stride = ls.mode_stride;
+  a.stage_limit = kStageSpinLimit;
   a.pos0 = d_pos0;
   a.vel0 = d_vel0;
   a.hit = nullptr;

@@ -139,15 +139,38 @@ __global__ void reduce_final(const cosims_traj_out *__restrict__ recs, long long
     s.n_hit = s_hit[0];
     s.n_success = s_succ[0];
     s.n_eff = n - fails;
-    s.steps = (int64_t)counters[C_STEPS];
-    s.force_evals = (int64_t)counters[C_FORCE_EVALS];
-    s.pot_evals = (int64_t)counters[C_POT_EVALS];
-    s.pair_lj = (int64_t)counters[C_PAIR_LJ];
-    s.pair_es = (int64_t)counters[C_PAIR_ES];
-    s.pair_pot = (int64_t)counters[C_PAIR_POT];
-    s.far_terms = (int64_t)counters[C_FAR];
+    // work counters of the launch (NULL: a slice of a multi-integral launch,
+    // whose work is reported for the whole call)
+    s.steps = counters ? (int64_t)counters[C_STEPS] : 0;
+    s.force_evals = counters ? (int64_t)counters[C_FORCE_EVALS] : 0;
+    s.pot_evals = counters ? (int64_t)counters[C_POT_EVALS] : 0;
+    s.pair_lj = counters ? (int64_t)counters[C_PAIR_LJ] : 0;
+    s.pair_es = counters ? (int64_t)counters[C_PAIR_ES] : 0;
+    s.pair_pot = counters ? (int64_t)counters[C_PAIR_POT] : 0;
+    s.far_terms = counters ? (int64_t)counters[C_FAR] : 0;
     *out = s;
   }
+}
+
+// Adds one launch's work counters to a record's work fields (steps .. far
+// terms); zero_first clears the whole record first.
+__global__ void add_work_kernel(const unsigned long long *counters, cosims_ccs_sums *w,
+                                int zero_first) {
+  if (threadIdx.x != 0) return;
+  if (zero_first) memset(w, 0, sizeof *w);
+  w->steps += (int64_t)counters[C_STEPS];
+  w->force_evals += (int64_t)counters[C_FORCE_EVALS];
+  w->pot_evals += (int64_t)counters[C_POT_EVALS];
+  w->pair_lj += (int64_t)counters[C_PAIR_LJ];
+  w->pair_es += (int64_t)counters[C_PAIR_ES];
+  w->pair_pot += (int64_t)counters[C_PAIR_POT];
+  w->far_terms += (int64_t)counters[C_FAR];
+}
+
+int add_work_launch(const unsigned long long *counters, cosims_ccs_sums *d_work, int zero_first,
+                    void *stream) {
+  add_work_kernel<<<1, 32, 0, (cudaStream_t)stream>>>(counters, d_work, zero_first);
+  return (int)cudaGetLastError();
 }
 
 int64_t reduce_scratch_len(int64_t n) {

@@ -723,7 +723,7 @@ __device__ __forceinline__ long long exact_take(const Exact &x, const Handoff &h
     }
     if (got >= 0) {
       bool ok = false;
-      for (uint32_t spin = 0; spin < (1u << 22); ++spin) {
+      for (uint32_t spin = 0; spin < ho.spin_limit; ++spin) {
         if (atomicAdd(ho.ready + got, 0u) != 0u) { ok = true; break; }
       }
       if (!ok) {
@@ -872,7 +872,7 @@ __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
   __shared__ uint64_t bar;
   const unsigned char *base = a.img.gbase;
   if (a.use_smem) {
-    if (!stage_to_smem(smem, a.img.gbase, a.img.bytes, &bar, 0, true)) {
+    if (!stage_to_smem(smem, a.img.gbase, a.img.bytes, &bar, 0, true, a.stage_limit)) {
       if (threadIdx.x == 0) atomicOr(a.counters + C_ERROR, 1ull);
       return;
     }
@@ -1023,7 +1023,7 @@ __global__ void __launch_bounds__(128) traj_plain_kernel(const TrajArgs a) {
         R.t = t; R.total = total; R.orbits = orbits; R.step = step; R.phase = phase;
         R.etries = (int32_t)etries; R.otries = (int32_t)otries; R.may_handoff = 0;
         __threadfence();
-        atomicExch(a.ho.ready + r, 1u);
+        if (!(a.ho.withhold_first && r == 0)) atomicExch(a.ho.ready + r, 1u);
         phase = P_ACQUIRE;
       }
     }

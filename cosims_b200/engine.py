@@ -58,6 +58,10 @@ def lib():
                                                    C.c_int64, V, V]),
                 "cosims_sample_inputs": (st, [V, C.c_uint64, C.c_int64, C.c_int64, V, V, V, V,
                                               V]),
+                "cosims_run_integrals": (st, [V, C.c_uint64, C.c_int64, C.c_int64, C.c_int32,
+                                              C.c_int64, V, V, V]),
+                "cosims_run_integrals_device": (st, [V, C.c_uint64, C.c_int64, C.c_int64,
+                                                     C.c_int32, C.c_int64, V, V, V]),
                 "cosims_batch_create": (st, [V, V, C.c_int32, C.c_int32, C.c_int32, P(V)]),
                 "cosims_batch_destroy": (None, [V]),
                 "cosims_batch_autotune": (st, [V, V]),
@@ -69,6 +73,7 @@ def lib():
                 "cosims_ctx_kernel_ms": (st, [V, P(C.c_float)]),
                 "cosims_ctx_kernel_timeline": (st, [V, P(C.c_double), P(C.c_double)]),
                 "cosims_ctx_set_handoff": (st, [V, C.c_int64, C.c_int32]),
+                "cosims_ctx_set_wait_test": (st, [V, C.c_uint32, C.c_uint32]),
                 "cosims_ctx_get_handoff": (st, [V, P(C.c_int64), P(C.c_int32), P(C.c_int64),
                                                 P(C.c_int64), P(C.c_double)]),
                 "cosims_serve_create": (st, [C.c_int32, C.c_int64, C.c_int32, C.c_int64, P(V)]),
@@ -204,6 +209,31 @@ class Context:
                            d_sums: int, stream=None) -> None:
         check(lib().cosims_run_sampled_device(self._h, seed, first, n, update_every,
                                               C.c_void_p(d_sums), _stream_ptr(stream)))
+
+    def run_integrals(self, seed: int, first: int, n_per: int, n_integrals: int,
+                      update_every: int = 0, stream=None) -> tuple:
+        """n_integrals CCS integrals of n_per trajectories each (integral k is
+        trajectories first + k * n_per ...), in as few launches as possible.
+        Returns (list of per-integral sums, the call's work counters)."""
+        recs = (abi.CcsSums * max(n_integrals, 1))()
+        work = abi.CcsSums()
+        check(lib().cosims_run_integrals(self._h, seed, first, n_per, n_integrals, update_every,
+                                         C.cast(recs, C.c_void_p), C.byref(work),
+                                         _stream_ptr(stream)))
+        return [recs[k] for k in range(n_integrals)], work
+
+    def run_integrals_device(self, seed: int, first: int, n_per: int, n_integrals: int,
+                             update_every: int, d_sums: int, d_work: int = 0,
+                             stream=None) -> None:
+        check(lib().cosims_run_integrals_device(self._h, seed, first, n_per, n_integrals,
+                                                update_every, C.c_void_p(d_sums),
+                                                C.c_void_p(d_work) if d_work else None,
+                                                _stream_ptr(stream)))
+
+    def set_wait_test(self, flags: int = 0, spin_limit: int = 0) -> None:
+        """Make the bounded device waits give up on purpose (tests of the
+        error path; abi.WAIT_TEST_* flags, 0 restores normal runs)."""
+        check(lib().cosims_ctx_set_wait_test(self._h, int(flags), int(spin_limit)))
 
     def kernel_ms(self) -> float:
         """Device time of the last trajectory-kernel launch (CUDA events)."""

@@ -250,7 +250,15 @@ static cosims_status setup_create(const cosims_config *cfg, const char *mol_path
   if (!ok) {
     log.copy_to(log_out, log_cap);
     delete s;
-    return fail(COSIMS_ERR_IO, "cannot read molecule file %s", mol_path);
+    // the reader's last error line says what is wrong with the file
+    std::string why;
+    const size_t at = log.text.rfind("Error");
+    if (at != std::string::npos) {
+      why = log.text.substr(at);
+      why = why.substr(0, why.find('\n'));
+    }
+    return fail(COSIMS_ERR_IO, "cannot read molecule file %s%s%s", mol_path,
+                why.empty() ? "" : ": ", why.c_str());
   }
   double r_disp = cfg->dispersion_radius, r_mp = cfg->multipole_radius;
   if (!set_properties(raw, s->ff, s->flags, s->mol, r_disp, r_mp, cfg->dispersion_cutoff != 0,

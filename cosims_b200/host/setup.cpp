@@ -257,10 +257,25 @@ bool read_mfj(const std::string &path, const std::vector<FFEntry> &ff, RawMolecu
     return true;
   };
   while (next_record()) {
+    // a record whose numbers do not parse, or are not finite, is corrupt: the
+    // reference reads it unchecked (atof: 0 for a word, NaN for "nan") and
+    // would integrate a wrong or non-finite molecule; here it is an error
+    const size_t line_no = raw.atoms.size() + 1;
+    if (!numeric_token(sx) || !numeric_token(sy) || !numeric_token(sz) ||
+        !numeric_token(sm) || (calc && !numeric_token(sq))) {
+      log.printf("Error: MFJ atom record %zu is not five numbers (%s %s %s %s %s)\n", line_no,
+                 sx.c_str(), sy.c_str(), sz.c_str(), sm.c_str(), sq.c_str());
+      return false;
+    }
     RawAtom a;
     a.x = atof(sx.c_str()) * scale * unitConv;
     a.y = atof(sy.c_str()) * scale * unitConv;
     a.z = atof(sz.c_str()) * scale * unitConv;
+    if (!std::isfinite(a.x) || !std::isfinite(a.y) || !std::isfinite(a.z) ||
+        (calc && !std::isfinite(atof(sq.c_str())))) {
+      log.printf("Error: MFJ atom record %zu has a non-finite coordinate or charge\n", line_no);
+      return false;
+    }
     a.has_charge = true;
     if (fl.charged) {
       double q = uniform ? fl.total_charge / (double)header_atoms : atof(sq.c_str());
@@ -280,6 +295,10 @@ bool read_mfj(const std::string &path, const std::vector<FFEntry> &ff, RawMolecu
     raw.atoms.push_back(a);
   }
   if (calc) fl.total_charge = total;
+  if (structure < 0 && header_atoms > 0 && (int)raw.atoms.size() != header_atoms)
+    log.printf(" Warning: the MFJ header gives %d atoms; %zu complete atom records were read\n",
+               header_atoms, raw.atoms.size());
+  if (raw.atoms.empty()) log.printf("Error: MFJ file holds no atom records\n");
   return !raw.atoms.empty();
 }
 

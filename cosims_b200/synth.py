@@ -171,6 +171,17 @@ def config2_molecule(seed: int = 2000) -> SynthMolecule:
                          0.35, seed)
 
 
+# force keys of the single-molecule configurations (input_text's names): the
+# LJ cut-off for the 128- and 512-atom molecules (variants 5 and 3), the 12 A
+# multipole cut-off for the 3000-atom protein (variant 1)
+CONFIG_FORCE = {0: "cutoff", 1: "cutoff", 2: "multipole12"}
+
+
+def config_molecule(k: int) -> SynthMolecule:
+    """The molecule of single-molecule configuration k (0, 1 or 2)."""
+    return {0: config0_molecule, 1: config1_molecule, 2: config2_molecule}[k]()
+
+
 def config3_sizes(n_mol: int = 256, seed: int = 3000) -> np.ndarray:
     rng = np.random.Generator(np.random.PCG64(seed))
     n = np.exp(rng.normal(math.log(400.0), 0.9, size=n_mol))

@@ -207,6 +207,21 @@ cosims_status cosims_ctx_set_handoff(cosims_ctx *ctx, int64_t step_budget, int32
 cosims_status cosims_ctx_get_handoff(cosims_ctx *ctx, int64_t *step_budget, int32_t *wide_lanes,
                                      int64_t *parked, int64_t *wide_steps, double *wide_ms);
 
+/* Tests of the error path.  Every device wait of the trajectory kernels is
+ * bounded: a wait that gives up sets an error flag, the kernel returns, and
+ * the call returns COSIMS_ERR_TIMEOUT with the context still usable.  This
+ * makes the waits give up on purpose, without any fault: with
+ * COSIMS_WAIT_TEST_STAGING every CTA's wait for its shared-memory copy of the
+ * molecule gives up at once (each CTA then waits for its copies in flight to
+ * land and leaves); with COSIMS_WAIT_TEST_HANDOFF the first trajectory parked
+ * for the long-trajectory hand-off is never published, so the wide group that
+ * takes it waits on a flag that nothing sets and gives up after spin_limit
+ * polls (0: the default, 2^22), and that trajectory's record is not written.
+ * flags 0 restores normal runs.  No counterpart in the reference. */
+#define COSIMS_WAIT_TEST_STAGING 0x1u
+#define COSIMS_WAIT_TEST_HANDOFF 0x2u
+cosims_status cosims_ctx_set_wait_test(cosims_ctx *ctx, uint32_t flags, uint32_t spin_limit);
+
 /* Fixed-list form: integrate n given start states (pos0, vel0: 3n doubles each,
  * host memory) and write n results to out (host).  Replaces, per trajectory,
  * diffEqSolver::verletVel (diffEqSolver.cpp:81-211) as monteTraj.cpp:362-364
@@ -249,6 +264,27 @@ cosims_status cosims_run_sampled_device(cosims_ctx *ctx, uint64_t seed,
                                         int64_t first_index, int64_t n,
                                         int64_t update_every,
                                         cosims_ccs_sums *d_sums, void *stream);
+/* Several CCS integrals of one molecule, as monteTraj::runTraj runs its
+ * `iter` integrals of `traj` trajectories (monteTraj.cpp:294-388), in as few
+ * trajectory-kernel launches as possible: integral k is trajectories
+ * first_index + k*n_per .. first_index + (k+1)*n_per - 1 of the seed's
+ * stream, and its sums are bit for bit those of cosims_run_sampled on that
+ * range (every trajectory runs as it would alone; each integral is reduced on
+ * its own records).  One launch holds as many whole integrals as the
+ * hand-off's 2^22 records allow, so the long trajectories that end one
+ * integral overlap the next integrals' work instead of leaving SMs idle.
+ * sums: n_integrals records (host); work: optional host record that receives
+ * the call's work counters (steps .. far_terms; the CCS fields are 0), which
+ * the per-integral records leave at 0.  Blocks until done. */
+cosims_status cosims_run_integrals(cosims_ctx *ctx, uint64_t seed, int64_t first_index,
+                                   int64_t n_per, int32_t n_integrals, int64_t update_every,
+                                   cosims_ccs_sums *sums, cosims_ccs_sums *work, void *stream);
+/* Same with device-resident records (d_sums: n_integrals; d_work may be
+ * NULL); stream-ordered, no host sync. */
+cosims_status cosims_run_integrals_device(cosims_ctx *ctx, uint64_t seed, int64_t first_index,
+                                          int64_t n_per, int32_t n_integrals,
+                                          int64_t update_every, cosims_ccs_sums *d_sums,
+                                          cosims_ccs_sums *d_work, void *stream);
 /* Start states only: the sampler and the ellipsoid projection
  * (monteTraj.cpp:235-277) for trajectories first_index..first_index+n-1.
  * Host outputs; pos0/vel0 are 3n doubles; hit is n int32. */
@@ -335,16 +371,23 @@ cosims_status cosims_batch_counters(cosims_batch *b, cosims_ccs_sums *work, floa
 /* ---- serving: continuous batching of CCS jobs ---------------------------- */
 /* No counterpart in the reference (it computes one molecule per process).
  * Jobs are admitted while their device footprint fits the HBM budget and a
- * slot is free; each job's molecule and running sums stay on the device.  A
- * round integrates the next chunk of every running job that fits the
- * server's max_jobs * round_traj trajectory slots (submission order) in one
- * persistent launch, and retires jobs whose relative standard error reached
- * their target (or that reached max_traj).  A job's first chunk is round_traj
- * trajectories (or min_traj); later chunks are what its running error says it
- * still needs (+5 %, in multiples of round_traj, at most 16 round_traj).
- * Chunks are the next trajectories of the job's own stream and their sizes
- * follow from the job alone, so its result does not depend on the other
- * jobs. */
+ * slot is free; each job's molecule and running sums stay on the device (the
+ * molecule in an image arena allocated at creation: admission allocates no
+ * device memory and waits for no kernel).  A round integrates the next chunk
+ * of every runnable job that fits the server's max_jobs * round_traj
+ * trajectory slots (submission order) in one persistent launch, and retires
+ * jobs whose relative standard error reached their target (or that reached
+ * max_traj).  Up to three rounds are in flight at once on the server's own
+ * streams; a job is in at most one of them, so jobs that arrive, or finish a
+ * chunk, while rounds run start in the next round without waiting for the
+ * others.  A job's first chunk is round_traj trajectories (or min_traj);
+ * later chunks are what its running error says it still needs (+5 %, in
+ * multiples of round_traj, at most 16 round_traj).  Chunks are the next
+ * trajectories of the job's own stream and their sizes follow from the job
+ * alone, so its result does not depend on the other jobs or on timing.
+ * The HBM budget covers the round buffers (3 * max_jobs * round_traj * 76
+ * bytes) and the image arena (the rest, at most 4 GiB).  Calls on one server
+ * must be serialised by the caller. */
 typedef struct cosims_server cosims_server;
 
 #define COSIMS_JOB_RUNNING 1
@@ -366,8 +409,11 @@ void cosims_serve_destroy(cosims_server *s);
 cosims_status cosims_serve_submit(cosims_server *s, const cosims_molecule *mol,
                                   const cosims_params *par, uint64_t seed, double target_rel_se,
                                   int64_t min_traj, int64_t max_traj, int64_t *job_id);
-/* One round over all running jobs on `stream`; waits for it.  n_finished:
- * jobs that retired in this round. */
+/* Advances the server: takes the results of every round that has completed
+ * (retiring jobs), then launches a round of the runnable jobs when a round
+ * buffer is free; when it could do neither, waits up to 5 ms for a round to
+ * complete.  Rounds are ordered after the work queued on `stream` at the call
+ * (NULL: no ordering).  n_finished: jobs retired by this call. */
 cosims_status cosims_serve_step(cosims_server *s, void *stream, int32_t *n_finished);
 cosims_status cosims_serve_poll(cosims_server *s, int64_t job_id, cosims_job_status *out);
 /* Frees a job's device resources (its slot and footprint return to the pool). */

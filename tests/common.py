@@ -33,3 +33,17 @@ def load(name: str):
 def hits(d):
     sel = d["hit"] == 1
     return d["start_pos"][sel], d["start_vel"][sel]
+
+
+@functools.lru_cache(maxsize=None)
+def config_setup(k: int, device: int | None = None):
+    """(MoleculeArrays, Params) of benchmark configuration k (0: 128-atom
+    neutral, 1: 512-atom +2 ion, 2: 3000-atom +10 protein with the 12 A
+    multipole cut-off) after the reference setup.  `device` runs the boundary
+    ray march on that GPU (bit for bit the host's)."""
+    import tempfile
+    from cosims_b200 import host, synth
+    tmp = tempfile.mkdtemp(prefix="cosims_cfg_")
+    mp, ip = synth.write_case(tmp, synth.config_molecule(k), synth.CONFIG_FORCE[k])
+    st = host.setup_from_files(mp, ip, seed=7, device=device)
+    return st.mol, st.params

@@ -87,3 +87,26 @@ def test_run_is_independent_of_batching():
         _, _, b1 = ctx.run_sampled(seed=21, first=0, n=700, want_records=True)
         _, _, b2 = ctx.run_sampled(seed=21, first=700, n=1300, want_records=True)
     np.testing.assert_array_equal(a, np.concatenate([b1, b2]))
+
+
+@pytest.mark.parametrize("precision", [abi.PLAIN_F64, abi.MIXED])
+@pytest.mark.parametrize("name", ["c0_t5", "c1_t3"])
+def test_run_integrals_equals_separate_integrals(name, precision):
+    """cosims_run_integrals: integral k of one call is bit for bit a separate
+    cosims_run_sampled of trajectories first + k n .. (the same sums and n_eff),
+    and the call's work counters are the separate runs' summed."""
+    mol, par, _ = load(name)
+    n, k, first, every = 3000, 3, 500, 700
+    with engine.Context(mol, par, precision) as ctx:
+        many, work = ctx.run_integrals(seed=13, first=first, n_per=n, n_integrals=k,
+                                       update_every=every)
+        sep = [ctx.run_sampled(seed=13, first=first + i * n, n=n, update_every=every)[0]
+               for i in range(k)]
+    for a, b in zip(many, sep):
+        assert (a.sum, a.sum2, a.max_de_pct, a.n, a.n_hit, a.n_success, a.n_eff) == \
+            (b.sum, b.sum2, b.max_de_pct, b.n, b.n_hit, b.n_success, b.n_eff)
+        assert a.steps == 0 and a.pair_es == 0            # work is reported for the call
+    assert work.steps == sum(b.steps for b in sep)
+    assert work.force_evals == sum(b.force_evals for b in sep)
+    assert work.pair_lj + work.pair_es == sum(b.pair_lj + b.pair_es for b in sep)
+    assert work.sum == 0 and work.n == 0

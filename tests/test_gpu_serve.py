@@ -68,3 +68,21 @@ def test_retirement_reaches_target():
             srv.step()
         st = srv.poll(j)
         assert st.rel_se <= 0.01 and st.sums.n % 8192 == 0 and st.omega > 0
+
+
+def test_served_ccs_matches_plain_fp64():
+    """Each retired job's Omega against the plain FP64 form run over the same
+    trajectories of the job's stream (its seed, indices 0..n-1): within the
+    mixed form's 0.3 % bar, at the serving configuration's 0.5 % target."""
+    jobs = [(n, 70 + i) for i, n in enumerate(NAMES)]
+    done = _run(jobs, round_traj=8192, target=0.005, max_jobs=4)
+    for (name, seed), st in done.items():
+        mol, par, _ = load(name)
+        with engine.Context(mol, par, abi.PLAIN_F64) as ctx:
+            s, _, _ = ctx.run_sampled(seed, 0, int(st.sums.n))
+        assert s.n_hit == st.sums.n_hit
+        om = s.sum / s.n_eff
+        err = abs(st.omega - om) / om
+        print(f"{name}: served {st.omega:.3f} ({st.sums.n} trajectories) vs plain "
+              f"{om:.3f}: {100 * err:.3f} %")
+        assert err <= 3e-3
