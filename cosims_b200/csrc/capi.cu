@@ -113,8 +113,22 @@ cosims_status validate(const cosims_molecule *mol, const cosims_params *par) {
   return COSIMS_OK;
 }
 
+// Whether the plain form's branch-free division and square root apply to the
+// molecule: every value that enters a dividend is zero or of magnitude in
+// [2^-400, 2^400] (the force loops check the position-dependent operands).
+int fast_arith_ok(const cosims_molecule *m) {
+  auto in = [](double v) {
+    const double a = std::fabs(v);
+    return a == 0.0 || (a >= 0x1p-400 && a <= 0x1p400);
+  };
+  for (int i = 0; i < m->n_atoms; i++)
+    if (!in(m->charge[i]) || !in(m->sig6[i]) || !in(m->eps24m[i]) || !in(m->eps4[i])) return 0;
+  return 1;
+}
+
 DevParams make_dev_params(const cosims_params *p) {
   DevParams d;
+  std::memset(&d, 0, sizeof d);
   d.force_type = p->force_type;
   d.multipole_order = p->multipole_order;
   d.projection = p->projection;
@@ -373,21 +387,25 @@ cosims_status shape_for(bool plain, const MolImage &img, int G, int block_thread
       if (!ok) continue;
       t.block = block;
       int per_sm = 0;
-      int rc = plain ? plain_occupancy(block, t.smem, &per_sm)
+      int rc = plain ? plain_occupancy(force_type, block, t.smem, &per_sm)
                      : mixed_occupancy(force_type, t.use_smem, G, block, t.smem, &per_sm);
       if (rc != 0) {
         cudaGetLastError();             // a refused shared-memory size: try the next shape
         continue;
       }
       if (per_sm <= 0) continue;        // over the kernel's thread, register or smem limit
-      const int resident = per_sm * block * (t.use_smem ? 2 : 1);
+      // mixed form: a staged image counts double (one copy serves a CTA's many
+      // groups from shared memory); plain form: every lane of a warp reads the
+      // same atom, a broadcast that L1 serves as well, so the most resident
+      // threads win (the staged shape on a tie)
+      const int resident = per_sm * block * (t.use_smem && !plain ? 2 : 1);
       if (resident > best_resident) {
         best_resident = resident;
         t.grid = per_sm;                // CTAs per SM until the grid is sized below
         ls = t;
         found = true;
       }
-      if (per_sm > 0) break;            // staged works: no need to try unstaged
+      if (per_sm > 0 && !plain) break;  // staged works: no need to try unstaged
     }
   }
   if (!found) return fail(COSIMS_ERR_UNSUPPORTED, "molecule image does not fit in shared memory");
@@ -584,6 +602,7 @@ cosims_status cosims_ctx_create(const cosims_molecule *mol, const cosims_params 
   c->sm_count = sm;
   c->max_smem = smem;
   c->par = make_dev_params(par);
+  c->par.fast_arith = fast_arith_ok(mol);
   c->n_atoms = mol->n_atoms;
   build_images(mol, par, c->h64, c->h32);
   c->img64 = c->h64.img;

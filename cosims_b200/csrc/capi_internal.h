@@ -23,6 +23,7 @@ cosims_status fail(cosims_status s, const char *fmt, ...);
 cosims_status cuda_fail(cudaError_t e, const char *what);
 cosims_status validate(const cosims_molecule *mol, const cosims_params *par);
 DevParams make_dev_params(const cosims_params *p);
+int fast_arith_ok(const cosims_molecule *m);
 void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h64,
                   HostImage &h32);
 int mode_stride_for(const MolImage &img, int force_type);
@@ -41,7 +42,7 @@ struct DeviceGuard {
   ~DeviceGuard();
 };
 
-int plain_occupancy(int block, size_t smem, int *per_sm);
+int plain_occupancy(int force_type, int block, size_t smem, int *per_sm);
 int mixed_occupancy(int force_type, int use_smem, int group_lanes, int block, size_t smem,
                     int *per_sm);
 

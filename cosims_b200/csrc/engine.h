@@ -106,6 +106,11 @@ struct DevParams {
   double b_max, start_dist, g_min, g_max, vdist_a, vdist_norm, vdist_max;
   double ccs_const;
   int64_t max_steps;
+  // plain form: the molecule's values allow the branch-free division and
+  // square root (every charge, sigma^6 and LJ prefactor zero or of magnitude
+  // in [2^-400, 2^400]); set by the host
+  int32_t fast_arith;
+  int32_t pad;
 };
 
 // Device-side counters of one run (all 64-bit, summed with atomics).

@@ -11,11 +11,25 @@
 //
 // Set-up: the first call on a device looks up that device's copy of the
 // array with cudaGetSymbolAddress (the device must be current; the address is
-// cached per device).  That first call should come before any stream capture.
-// Every call shares the array and leaves its contents behind; the call clears
-// what must start at zero (queue, counters, histogram).  Calls that overlap
-// on the GPU -- two streams, or two host threads -- race on the array: run
-// them one after another.
+// cached per device, so the device's primary context -- the one the CUDA
+// runtime uses -- is the one supported).  That first call should come before
+// any stream capture.  Every call shares the array and leaves its contents
+// behind; the call clears what must start at zero (queue, counters,
+// histogram).  Calls that overlap on the GPU -- two streams, or two host
+// threads -- race on the array: run them one after another.
+//
+// The run has no long-trajectory hand-off (its records would need 200 bytes
+// per trajectory of scratch): every trajectory is integrated to its end by
+// the group that started it.  The mixed form's results are those of a context
+// with the hand-off off (cosims_ctx_set_handoff(ctx, -1, 0)); with the hand-off
+// on, a trajectory past its 2048-step budget is finished by a wide group whose
+// FP32 sums run in another order.  The plain form's results are bit for bit
+// the context's either way, but its longest trajectories then run on one
+// thread each, so a 1e5-trajectory call takes about 5x as long as with the
+// hand-off (1.3-1.6 s against 0.27 s for the 512-atom ion).
+//
+// The molecule images are copied from pageable host memory (the call may wait
+// for that copy before it returns).
 #include <cuda_runtime.h>
 #include <cstring>
 #include <mutex>
@@ -26,9 +40,11 @@ namespace cosims {
 
 namespace {
 
-constexpr size_t kNoallocScratchBytes = 8u << 20;        // 8 MiB per device
+constexpr size_t kNoallocScratchBytes = 12u << 20;       // 12 MiB per device
 constexpr size_t kCtrlBytes = 4096;                       // queue, counters, order scratch
-constexpr size_t kImageBytes = 2u << 20;                  // molecule images (F64 + F32)
+// molecule images (F64 + F32): about 100 bytes per atom and 340 per cluster,
+// so every molecule of the 16384-atom limit fits with up to 7500 clusters
+constexpr size_t kImageBytes = 4u << 20;
 constexpr size_t kOrderBytes = kNoallocScratchBytes - kCtrlBytes - kImageBytes;
 constexpr int64_t kNoallocMaxTraj = (int64_t)(kOrderBytes / sizeof(int32_t));
 constexpr int kMaxDevices = 64;
@@ -114,7 +130,8 @@ extern "C" cosims_status cosims_run_list_noalloc(const cosims_molecule *mol,
   if (e != cudaSuccess) return cuda_fail(e, "no-alloc staging");
   if (n == 0) return COSIMS_OK;
 
-  const DevParams dp = make_dev_params(par);
+  DevParams dp = make_dev_params(par);
+  dp.fast_arith = fast_arith_ok(mol);
   int rc = order_launch(dp, d_vel0, nullptr, n, order, order_scratch, stream);
   if (rc != 0) return cuda_fail((cudaError_t)rc, "work-order launch");
 

@@ -308,6 +308,16 @@ cosims_status cosims_ctx_kernel_timeline(cosims_ctx *ctx, double *drain_ms, doub
  * bound by these pipes rather than by HBM or the tensor cores. */
 cosims_status cosims_probe_peaks(int32_t device, double *fp32_tflops, double *fp64_tflops);
 
+/* Self-check of the branch-free FP64 division and square root that the plain
+ * form's force loops use in place of the IEEE operators (whose slow-path
+ * branches serialise the per-atom dependency chains): n operand pairs per
+ * call, drawn from `seed`, over the whole valid range, the force loops'
+ * physical ranges and mantissa edge cases; div_mismatches / sqrt_mismatches
+ * receive the results that differ from CUDA's `/` and `sqrt` in any bit (0
+ * expected).  No counterpart in the reference. */
+cosims_status cosims_check_exact_arith(int32_t device, uint64_t seed, int64_t n,
+                                       int64_t *div_mismatches, int64_t *sqrt_mismatches);
+
 /* ---- no device allocation ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot let this library
  * allocate device memory -- a host program that owns the GPU's memory through
@@ -316,16 +326,24 @@ cosims_status cosims_probe_peaks(int32_t device, double *fp32_tflops, double *fp
  * (as cosims_run_list_device) without a context and allocates nothing: the
  * caller passes the molecule and scalars (host), device buffers d_pos0 /
  * d_vel0 (3n doubles each) and d_out (n records); the molecule image, work
- * queue, work order and counters live in one static 8 MiB device array that
+ * queue, work order and counters live in one static 12 MiB device array that
  * every GPU loading this library holds until the process exits.  Limits: at
- * most 1,571,840 trajectories per call and a molecule image of at most 2 MiB
- * (every molecule within the 16384-atom limit fits); larger requests return
+ * most 2,096,128 trajectories per call and molecule images of at most 4 MiB
+ * (about 100 bytes per atom and 340 per cluster: every molecule within the
+ * 16384-atom limit fits with up to 7500 clusters); larger requests return
  * COSIMS_ERR_UNSUPPORTED before any device work.  The first call on a device
- * looks up its array (cudaGetSymbolAddress, with that device current) and
+ * looks up its array (cudaGetSymbolAddress, with that device current; the
+ * device's primary context, the CUDA runtime's, is the one supported) and
  * should come before any stream capture.  Calls share the array: calls that
  * overlap on the GPU (other streams or host threads) race; run them in turn.
- * Stream-ordered: returns without synchronising.  group_lanes: lanes per
- * trajectory of the mixed form (ignored by the plain form). */
+ * The run has no long-trajectory hand-off: mixed-form results equal a
+ * context's with cosims_ctx_set_handoff(ctx, -1, 0), and plain-form results
+ * are bit for bit the context's but its longest trajectories run on one
+ * thread each (about 5x the time of a context call on a 1e5-trajectory list).
+ * The molecule images are copied from pageable host memory, so the call may
+ * wait for that copy; otherwise it is stream-ordered and returns without
+ * synchronising.  group_lanes: lanes per trajectory of the mixed form
+ * (ignored by the plain form). */
 cosims_status cosims_run_list_noalloc(const cosims_molecule *mol, const cosims_params *par,
                                       int32_t precision, int32_t group_lanes,
                                       const double *d_pos0, const double *d_vel0, int64_t n,

@@ -19,7 +19,7 @@ from tests.common import hits, load
 pytestmark = pytest.mark.gpu
 
 CHI_TOL = 1e-12          # as tests/test_gpu_plain.py
-MAX_TRAJ = 1_571_840     # the documented per-call limit
+MAX_TRAJ = 2_096_128     # the documented per-call limit
 
 
 def _noalloc():
@@ -67,3 +67,56 @@ def test_noalloc_rejects_sizes_beyond_its_limit():
                     None, None)
     assert rc == abi.ERR_UNSUPPORTED
     assert b"no-alloc limit" in engine.lib().cosims_last_error()
+
+
+def test_noalloc_rejects_a_molecule_image_beyond_its_limit():
+    """16000 atoms in 16000 one-atom clusters need about 7 MB of images, more
+    than the 4 MiB the array holds for them."""
+    mol, par, _ = load("c0_t5")
+    n = 16000
+    rng = np.random.default_rng(3)
+    xyz = rng.normal(0.0, 30.0, size=(n, 3))
+    big = abi.MoleculeArrays(
+        xyz=xyz, charge=np.zeros(n), sig6=np.full(n, mol.sig6[1]),
+        eps24m=np.full(n, mol.eps24m[1]), eps4=np.full(n, mol.eps4[1]),
+        cluster_offset=np.arange(n + 1, dtype=np.int32),
+        cluster_atoms=np.arange(n, dtype=np.int32), cluster_pos=xyz,
+        cluster_radius=np.zeros(n), cluster_charge=np.zeros(n),
+        cluster_dipole=np.zeros((n, 3)), cluster_quad=np.zeros((n, 9)),
+        cluster_replaced=np.zeros(n, np.int32))
+    view = big.view()
+    rc = _noalloc()(C.byref(view), C.byref(par), abi.PLAIN_F64, 1, None, None, 0, None, None)
+    assert rc == abi.ERR_UNSUPPORTED
+    assert b"no-alloc limit" in engine.lib().cosims_last_error()
+
+
+def test_noalloc_runs_without_handoff():
+    """The path has no long-trajectory hand-off.  On a mixed-form list that
+    holds trajectories past the context's 2048-step budget, its results are bit
+    for bit those of a context with the hand-off off."""
+    import torch
+    mol, par, _ = load("c1_t3")
+    lanes = 8
+    with engine.Context(mol, par, abi.MIXED) as ctx:
+        ctx.set_launch(group_lanes=lanes)
+        ctx.set_handoff(-1, 0)
+        _, p0, v0, hit = ctx.sample_inputs(seed=2, first=0, n=40000)
+        p0, v0 = p0[hit == 1], v0[hit == 1]
+        scan = ctx.run_list(p0, v0)
+        long_ = np.flatnonzero(scan["steps"] > 2048)
+        assert long_.size > 0, "no trajectory past 2048 steps in the sample"
+        sel = np.concatenate([np.arange(300), long_])
+        p0, v0 = np.ascontiguousarray(p0[sel]), np.ascontiguousarray(v0[sel])
+        ref = ctx.run_list(p0, v0)
+    n = p0.shape[0]
+    dp0 = torch.from_numpy(p0).cuda()
+    dv0 = torch.from_numpy(v0).cuda()
+    dout = torch.empty(n * abi.TRAJ_OUT_DTYPE.itemsize, dtype=torch.uint8, device="cuda")
+    view = mol.view()
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    engine.check(_noalloc()(C.byref(view), C.byref(par), abi.MIXED, lanes, dp0.data_ptr(),
+                            dv0.data_ptr(), n, dout.data_ptr(), stream))
+    torch.cuda.synchronize()
+    out = np.frombuffer(dout.cpu().numpy().tobytes(), dtype=abi.TRAJ_OUT_DTYPE)
+    np.testing.assert_array_equal(out, ref)
+    assert (out["steps"] > 2048).any()
