@@ -731,6 +731,9 @@ def main():
                     help="hand-off step budget of the profiled run (0: the default; < 0: off)")
     ap.add_argument("--profile-max-steps", type=int, default=0,
                     help="step cap of the profiled run's trajectories (0: the default)")
+    ap.add_argument("--profile-config", type=int, default=1, choices=[0, 1, 2],
+                    help="molecule of the profiled run: 0 the 128-atom neutral molecule, "
+                         "1 the 512-atom ion (default), 2 the 3000-atom protein")
     ap.add_argument("--group-lanes", type=int, default=0)
     ap.add_argument("--workload", choices=["integral", "batched", "serving", "protein", "small"],
                     default="integral",
@@ -779,6 +782,12 @@ def main():
     mol, par = st.mol, st.params
     stream = torch.cuda.current_stream()
     if args.profile:
+        if args.profile_config != 1:
+            from cosims_b200 import synth
+            k = args.profile_config
+            mp_k, ip_k = synth.write_case(tmp, synth.config_molecule(k), synth.CONFIG_FORCE[k])
+            st = host.setup_from_files(mp_k, ip_k, seed=SEED, device=local)
+            mol, par = st.mol, st.params
         profile_case(args, mol, par, stream, torch)
         return
     d_sums = torch.zeros(1024, dtype=torch.uint8, device="cuda")

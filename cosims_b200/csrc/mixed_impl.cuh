@@ -349,11 +349,12 @@ struct NarrowLanes {
   }
   // float sums of 16- and 32-lane groups: reduce-scatter, then each lane
   // fetches every value from a lane that holds it (P/2 + ... + K shuffles
-  // instead of K log2(G)); other widths use the butterfly
+  // instead of K log2(G); the 22 sums of the far-field variants on 32 lanes:
+  // 31 + 22 instead of 110); other widths use the butterfly
   template <int K>
   __device__ __forceinline__ void sum(float (&v)[K]) {
     constexpr int P = PowTwo<K>::P;
-    if (K > 2 && P <= 16 && (G == 16 || G == 32)) {
+    if (K > 2 && P <= G && (G == 16 || G == 32)) {
       int idx;
       const float r = reduce_scatter<K>(v, G, lane, idx);
       const int gbase = (threadIdx.x & 31) & ~(G - 1);
@@ -422,14 +423,16 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     }
     fold<TYPE>(t, s);
   } else if (Traits<TYPE>::kListed) {
-    // pass 1: near/far decision per cluster (FP64), far-field terms; the
-    // clusters that add pair terms go into the group's list (cluster << 8 |
-    // mode), compacted by ballot, so pass 2 skips the rest as the reference
-    // does (forceAccel.cpp:221-633, 807-854)
+    // pass 1: near/far decision per cluster (FP64).  The clusters that add
+    // pair terms go into the group's list (cluster << 8 | mode), compacted by
+    // ballot: those with the charge field from the front, the LJ-only ones
+    // from the back, so pass 2 skips the rest as the reference does
+    // (forceAccel.cpp:221-633, 807-854) and packs pairs of one kind.
     uint32_t *list = reinterpret_cast<uint32_t *>(modes);
     const int gbase = (threadIdx.x & 31) & ~(G - 1);
     const unsigned gbits = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
-    int count = 0;
+    const unsigned below = (1u << lane) - 1u;
+    int n_es = 0, n_lj = 0;
     for (int c0 = 0; c0 < m.nc; c0 += G) {
       const int c = c0 + lane;
       uint32_t mode = 0;
@@ -441,7 +444,6 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         if (TYPE == 5) {
           mode = in_disp ? M_LJ : 0;
         } else if (r2 > C.mpr2) {
-          far_terms(m, c, p.multipole_order, (float)d0, (float)d1, (float)d2, s);
           w.far++;
           mode = TYPE == 2 ? M_LJ : (in_disp ? M_LJQ : 0);
         } else {
@@ -451,41 +453,65 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         if (mode & M_ES) w.es += cnt;
         else if (mode) w.lj += cnt;
       }
-      const unsigned mine = (__ballot_sync(0xffffffffu, mode != 0) >> gbase) & gbits;
-      if (mode != 0) list[count + __popc(mine & ((1u << lane) - 1u))] = ((uint32_t)c << 8) | mode;
-      count += __popc(mine);
+      const bool es = (mode & M_ES) != 0, ljo = mode != 0 && !es;
+      const unsigned m_es = (__ballot_sync(0xffffffffu, es) >> gbase) & gbits;
+      const unsigned m_lj = (__ballot_sync(0xffffffffu, ljo) >> gbase) & gbits;
+      const uint32_t e = ((uint32_t)c << 8) | mode;
+      if (es) list[n_es + __popc(m_es & below)] = e;
+      if (ljo) list[m.nc - 1 - n_lj - __popc(m_lj & below)] = e;
+      n_es += __popc(m_es);
+      n_lj += __popc(m_lj);
     }
     ln.sync();
-    // pass 2: the listed clusters' atoms; with 32 lanes two clusters at a time
-    // (clusters hold at most a few tens of atoms)
+    // pass 2: the listed clusters, two at a time per (half-)group in the two
+    // halves of the packed instructions: lane `sub` takes atom sub (+16 ...)
+    // of both; a cluster without a partner, or the shorter of the two, is
+    // padded in registers with an inert atom (zero charge and prefactor, 1e6 A
+    // away), whose terms are exactly zero
     const int split = G == 32 ? 16 : G;
     const int sub = lane & (split - 1), half = G == 32 ? (lane >> 4) : 0;
     const int step = G == 32 ? 2 : 1;
     Acc2 t = {};
     const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
     const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
-    for (int i = half; i - half < count; i += step) {
-      if (i < count) {
-        const uint32_t e = list[i];
-        const ClusterF32 &C = m.cl[e >> 8];
-        const uint32_t mode = e & 0xffu;
-        const bool es = (mode & M_ES) != 0;
-        int k = C.a0 + sub;
-        // two atoms of the cluster at once (not for the far-field variants,
-        // whose 22 scalar sums leave no registers for the packed ones)
-        for (; !Traits<TYPE>::kFar && k + split < C.a1; k += 2 * split) {
-          const float4 a0 = m.a4[k], b0 = m.b4[k], a1 = m.a4[k + split], b1 = m.b4[k + split];
-          const float2 p0 = lj_params<TYPE>(m, b0, mode), p1 = lj_params<TYPE>(m, b1, mode);
-          pair2<TYPE>(a0, a1, f2(p0.x, p1.x), f2(p0.y, p1.y), es, hx2, hy2, hz2, lx2, ly2, lz2,
-                      t);
-        }
-        for (; k < C.a1; k += split) {
-          const float4 a = m.a4[k], b = m.b4[k];
-          pair<TYPE>(m, a, b, mode, hx, hy, hz, lx, ly, lz, s, &C);
+    const float4 inert_a = make_float4(hx + 1.0e6f, hy, hz, 0.0f);
+    const float4 inert_b = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    auto params = [&](const ClusterF32 &C, const float4 &b, uint32_t mode) {
+      if (TYPE == 1 && (mode & M_LJQ)) return f2(C.qsig6, C.qeps);
+      return f2(b.x, (mode & (M_LJ | M_LJQ)) ? b.y : 0.0f);
+    };
+    auto run_pairs = [&](int lo, int hi, bool es) {
+      for (int i = lo + 2 * half; i < hi; i += 2 * step) {
+        const uint32_t ea = list[i];
+        const bool has_b = i + 1 < hi;
+        const uint32_t eb = has_b ? list[i + 1] : ea;
+        const ClusterF32 &CA = m.cl[ea >> 8];
+        const ClusterF32 &CB = m.cl[eb >> 8];
+        const int na = CA.a1 - CA.a0, nb = has_b ? CB.a1 - CB.a0 : 0;
+        const int nmax = na > nb ? na : nb;
+        for (int k = sub; k < nmax; k += split) {
+          const bool ia = k < na, ib = k < nb;
+          const float4 a0 = ia ? m.a4[CA.a0 + k] : inert_a, b0 = ia ? m.b4[CA.a0 + k] : inert_b;
+          const float4 a1 = ib ? m.a4[CB.a0 + k] : inert_a, b1 = ib ? m.b4[CB.a0 + k] : inert_b;
+          const float2 p0 = params(CA, b0, ea & 0xffu), p1 = params(CB, b1, eb & 0xffu);
+          pair2<TYPE>(a0, a1, f2(ia ? p0.x : 0.0f, ib ? p1.x : 0.0f),
+                      f2(ia ? p0.y : 0.0f, ib ? p1.y : 0.0f), es, hx2, hy2, hz2, lx2, ly2, lz2, t);
         }
       }
-    }
+    };
+    if (Traits<TYPE>::kCharge) run_pairs(0, n_es, true);
+    run_pairs(m.nc - n_lj, m.nc, false);
     fold<TYPE>(t, s);
+    // pass 3: the far field of the far clusters (multipole variants), after the
+    // pair sums are folded, so the pair loop keeps its registers for them
+    if (Traits<TYPE>::kFar) {
+      for (int c = lane; c < m.nc; c += G) {
+        const ClusterF32 &C = m.cl[c];
+        const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
+        const double r2 = d0 * d0 + d1 * d1 + d2 * d2;
+        if (r2 > C.mpr2) far_terms(m, c, p.multipole_order, (float)d0, (float)d1, (float)d2, s);
+      }
+    }
     ln.sync();
   } else if (Traits<TYPE>::kClusters) {
     // pass 1: near/far decision per cluster (FP64), far-field terms

@@ -7,7 +7,7 @@
  * evaluation order, so that for the same inputs the results agree bit for bit
  * with the reference compiled by g++ on x86-64 (SSE2, no FMA).  That claim is
  * checked against oracle/_ref (the reference's own code) by
- * tests/test_oracle_vs_reference.py and through tests/golden fixtures.
+ * tests/test_oracle_golden.py through the tests/golden fixtures.
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg use
  * this file, as the checker.  The product never calls it.

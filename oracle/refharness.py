@@ -19,7 +19,10 @@ from cosims_b200 import abi
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_ref", "libcosims_ref.so")
 BIN_PATH = os.path.join(HERE, "_ref", "cosims")
-REF_ROOT = os.environ.get("COSIMS_REF", "/root/reference")
+# the CoSIMS checkout: $COSIMS_REF, else the directory `reference` beside this
+# repository
+REF_ROOT = os.environ.get("COSIMS_REF") or os.path.normpath(
+    os.path.join(HERE, "..", "..", "reference"))
 
 # order of ref_get_scalars (ref_harness.cpp)
 SCALARS = ("mu totalMass beta g_min g_max vdist_max vdist_norm ell_a ell_b ell_c b_max "

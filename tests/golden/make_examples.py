@@ -16,7 +16,7 @@ reference's setup, tests/test_host_setup.py), the run settings of the input
 (trajectories per integral, integrals, progress interval) and the published
 weighted CCS and error, read from the log.  Run it where the checkout is:
 
-    COSIMS_REF=<path of the CoSIMS checkout> python tests/golden/make_examples.py
+    python tests/golden/make_examples.py   (checkout: $COSIMS_REF, else ../reference)
 """
 from __future__ import annotations
 
@@ -59,9 +59,9 @@ def published(log_path: str) -> tuple:
 
 
 def main() -> None:
-    ref = os.environ.get("COSIMS_REF")
-    if not ref:
-        sys.exit("set COSIMS_REF to the CoSIMS checkout")
+    from oracle.refharness import REF_ROOT as ref      # $COSIMS_REF or ../reference
+    if not os.path.isdir(os.path.join(ref, "examples")):
+        sys.exit(f"no CoSIMS checkout at {ref}: set COSIMS_REF")
     ex = os.path.join(ref, "examples")
     for name, (mol, inp, atoms, log) in EXAMPLES.items():
         mp = os.path.join(ex, mol)

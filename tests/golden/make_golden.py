@@ -1,7 +1,7 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Run where the CoSIMS reference checkout is available (default
-/root/reference, or $COSIMS_REF):
+Run where the CoSIMS reference checkout is available ($COSIMS_REF, else the
+directory `reference` beside this repository):
 
     python tests/golden/make_golden.py
 

@@ -13,7 +13,7 @@ import pytest
 from cosims_b200 import abi, host, synth
 from tests.common import load
 
-REF = os.environ.get("COSIMS_REF", "/root/reference")
+from oracle.refharness import REF_ROOT as REF  # noqa: E402  ($COSIMS_REF or ../reference)
 EX = os.path.join(REF, "examples")
 has_ref = pytest.mark.skipif(not os.path.isdir(EX), reason="reference checkout not present")
 
