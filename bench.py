@@ -333,6 +333,7 @@ def setup_library(mols, device: int):
     from cosims_b200 import host, synth
     tmp = tempfile.mkdtemp(prefix="cosims_lib_")
     out, each = [], []
+    phases = [0.0] * 6
     t0 = time.time()
     for m in mols:
         t1 = time.perf_counter()
@@ -341,8 +342,12 @@ def setup_library(mols, device: int):
         st = host.setup_from_files(mp_, ip, seed=SEED, device=device)
         out.append((st.mol, st.params))
         each.append(time.perf_counter() - t1)
+        phases = [a + b for a, b in zip(phases, list(st.info.setup_ms))]
     shutil.rmtree(tmp, ignore_errors=True)
-    return out, time.time() - t0, each
+    names = ("read", "properties_rotation", "velocity_distribution", "boundary_scan_gpu",
+             "ellipsoid_fit", "pcm_clusters")
+    split = {k: round(v / len(mols), 3) for k, v in zip(names, phases)}
+    return out, time.time() - t0, each, split
 
 
 def batched_block(args, local, torch, steps: int, warmup: int, library=None) -> dict:
@@ -357,9 +362,9 @@ def batched_block(args, local, torch, steps: int, warmup: int, library=None) -> 
     if library is None:
         mols, sizes = config3_library(args.molecules)
         gen_s = time.time() - t0
-        lib_, setup_s, _ = setup_library(mols, local)
+        lib_, setup_s, _, split = setup_library(mols, local)
     else:
-        lib_, sizes, gen_s, setup_s, _ = library
+        lib_, sizes, gen_s, setup_s, _, split = library
     ms_, pars = [m for m, _ in lib_], [p for _, p in lib_]
     k = len(ms_)
     stream = torch.cuda.current_stream()
@@ -446,6 +451,7 @@ def batched_block(args, local, torch, steps: int, warmup: int, library=None) -> 
                      "kernel": "batch_mixed_kernel", "kernel_ms": sum(kern_ms) / len(kern_ms)},
         "host_s": {"generate": round(gen_s, 1), "setup": round(setup_s, 1),
                    "autotune": round(tune_s, 1)},
+        "setup_ms_per_molecule_by_phase": split,
         "clocks": clk,
     }
 
@@ -501,9 +507,9 @@ def serving_block(args, local, torch, library=None, duration: float | None = Non
     duration = args.duration if duration is None else duration
     if library is None:
         mols, sizes = config3_library(args.molecules)
-        lib_, setup_s, per_setup = setup_library(mols, local)
+        lib_, setup_s, per_setup, _ = setup_library(mols, local)
     else:
-        lib_, sizes, _, setup_s, per_setup = library
+        lib_, sizes, _, setup_s, per_setup, _ = library
     rng = np.random.Generator(np.random.PCG64(SEED))
     round_traj = 8192
     srv = engine.Server(device=local, hbm_budget=16 << 30, max_jobs=128, round_traj=round_traj)
@@ -709,8 +715,8 @@ def library_for_extras(args, local):
     t0 = time.time()
     mols, sizes = config3_library(args.molecules)
     gen_s = time.time() - t0
-    lib_, setup_s, per = setup_library(mols, local)
-    return lib_, sizes, gen_s, setup_s, per
+    lib_, setup_s, per, split = setup_library(mols, local)
+    return lib_, sizes, gen_s, setup_s, per, split
 
 
 def main():

@@ -54,6 +54,7 @@ class SetupInfo(C.Structure):
         ("r_mp", C.c_double),
         ("centers_replaced", C.c_int32),
         ("avg_cluster_size", C.c_double), ("avg_cluster_radius", C.c_double),
+        ("setup_ms", C.c_double * 6),
     ]
 
     def as_dict(self) -> dict:

@@ -2,6 +2,7 @@
 // parameters and the per-molecule setup sequence of monteTraj::monteTraj.
 #include <algorithm>
 #include <cctype>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <fstream>
@@ -220,6 +221,14 @@ static cosims_status setup_create(const cosims_config *cfg, const char *mol_path
                                   char *log_out, int64_t log_cap, cosims_setup **out) {
   if (!cfg || !mol_path || !out) return fail(COSIMS_ERR_INVALID, "config, molecule and out are required");
   *out = nullptr;
+  // wall time of the setup phases (cosims_setup_info::setup_ms)
+  double phase_ms[6] = {0, 0, 0, 0, 0, 0};
+  auto clock = std::chrono::steady_clock::now();
+  auto lap = [&](int k) {
+    const auto now = std::chrono::steady_clock::now();
+    phase_ms[k] += std::chrono::duration<double, std::milli>(now - clock).count();
+    clock = now;
+  };
   Log log;
   cosims_setup *s = new cosims_setup();
   s->cfg = *cfg;
@@ -260,6 +269,7 @@ static cosims_status setup_create(const cosims_config *cfg, const char *mol_path
     return fail(COSIMS_ERR_IO, "cannot read molecule file %s%s%s", mol_path,
                 why.empty() ? "" : ": ", why.c_str());
   }
+  lap(0);
   double r_disp = cfg->dispersion_radius, r_mp = cfg->multipole_radius;
   if (!set_properties(raw, s->ff, s->flags, s->mol, r_disp, r_mp, cfg->dispersion_cutoff != 0,
                       cfg->multipole != 0, log)) {
@@ -268,6 +278,7 @@ static cosims_status setup_create(const cosims_config *cfg, const char *mol_path
     return fail(COSIMS_ERR_IO, "unknown atom type in %s", mol_path);
   }
   rotate_to_inertia_frame(s->mol, log);
+  lap(1);
   Molecule &m = s->mol;
   const bool charged = s->flags.charged;
   // monteTraj::monteTraj (monteTraj.cpp:31-94)
@@ -283,6 +294,7 @@ static cosims_status setup_create(const cosims_config *cfg, const char *mol_path
   const double maxVelDistr = std::pow(mode, distrPower) * std::exp(-va * mode * mode) * norm;
   const double dipole_scalar = kDipoleScalar / mu;
   const double minKin = 0.5 * mu * std::pow(vd_mean(2, beta / 2.0) - 2 * vd_std(2, beta / 2.0), 2);
+  lap(2);
   int threads = cfg->threads > 0 ? cfg->threads : 1;
   if (threads == 1) threads = std::max(1u, std::thread::hardware_concurrency());
   if (!boundary_scan(m, charged, dipole_scalar, minKin, threads, device, s->boundary, log)) {
@@ -290,9 +302,11 @@ static cosims_status setup_create(const cosims_config *cfg, const char *mol_path
     delete s;
     return fail(COSIMS_ERR_INVALID, "potential-energy boundary scan failed");
   }
+  lap(3);
   fit_ellipsoid(s->boundary, s->ell);
   Ellipsoid fitted = s->ell;
   enlarge_ellipsoid(s->boundary, s->ell);
+  lap(4);
   const double bMax = std::max(s->ell.a, std::max(s->ell.b, s->ell.c));   // impactParam.cpp:417
   // forceAccel::setClusters (forceAccel.cpp:63-140)
   const bool clusters = cfg->multipole || cfg->dispersion_cutoff;
@@ -301,6 +315,7 @@ static cosims_status setup_create(const cosims_config *cfg, const char *mol_path
     delete s;
     return fail(COSIMS_ERR_INVALID, "cluster formation failed");
   }
+  lap(5);
   int force_type;
   if (charged)
     force_type = cfg->multipole ? (cfg->dispersion_cutoff ? 1 : 2)
@@ -380,6 +395,7 @@ static cosims_status setup_create(const cosims_config *cfg, const char *mol_path
   in.centers_replaced = s->cl.n_replaced;
   in.avg_cluster_size = s->cl.avg_size;
   in.avg_cluster_radius = s->cl.avg_radius;
+  for (int k = 0; k < 6; k++) in.setup_ms[k] = phase_ms[k];
   s->info.n_clusters = in.n_clusters;
   // axes of the fit before enlargement are kept in fitted; the path uses the enlarged ones
   (void)fitted;

@@ -89,6 +89,10 @@ typedef struct cosims_setup_info {
     double beta, ccs_const, r_disp, r_mp;
     int32_t centers_replaced;
     double avg_cluster_size, avg_cluster_radius;
+    /* wall time (ms) of the setup phases: molecule file, force-field terms and
+     * rotation, velocity distribution, boundary scan, ellipsoid fit and
+     * enlargement, PCM clusters and multipoles */
+    double setup_ms[6];
 } cosims_setup_info;
 
 /* The whole per-molecule setup.  atom_path: optional atoms.dat (NULL or "").
