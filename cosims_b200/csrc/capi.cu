@@ -325,9 +325,9 @@ static cosims_status grow(T **p, int64_t *cap, int64_t need) {
 int mode_stride_for(const MolImage &img, int force_type) {
   if (!img.uses_clusters) return 0;
   // variants 1, 2, 5 keep a 4-byte entry per cluster (the list of clusters
-  // that add pair terms); the others one mode byte per cluster, plus the pad
-  // atoms' cluster
-  const int per = (force_type == 1 || force_type == 2 || force_type == 5) ? 4 : 1;
+  // that add pair terms) and variant 3 a 4-byte cut-off factor per cluster;
+  // the others one mode byte per cluster; plus the pad atoms' cluster
+  const int per = (force_type == 1 || force_type == 2 || force_type == 3 || force_type == 5) ? 4 : 1;
   int s = ((img.n_clusters + 1) * per + 3) & ~3;
   if (((s / 4) & 1) == 0) s += 4;     // odd word count: groups hit distinct banks
   return s;

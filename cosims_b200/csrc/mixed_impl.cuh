@@ -379,10 +379,13 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
   const float lx = (float)(pos[0] - (double)hx), ly = (float)(pos[1] - (double)hy),
               lz = (float)(pos[2] - (double)hz);
   if (Traits<TYPE>::kMaskable && m.nc < 64) {
-    // variants 3 and 5 with fewer than 64 clusters: the cut-off decision of
-    // every cluster in one register (ballot per round of G clusters), no
-    // shared-memory lookup per atom
+    // variant 3 with fewer than 64 clusters: the cut-off decision of every
+    // cluster in one register (ballot per round of G clusters) and, for the
+    // pair loop, as a factor 1 or 0 per cluster in the group's scratch (one
+    // shared load and a packed multiply per slot pair instead of 64-bit bit
+    // tests and selects)
     unsigned long long in_mask = 0;
+    float *fac = reinterpret_cast<float *>(modes);
     const int gbase = (threadIdx.x & 31) & ~(G - 1);
     const unsigned gbits = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
     for (int c0 = 0; c0 < m.nc; c0 += G) {
@@ -393,10 +396,12 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
         in = !(d0 * d0 + d1 * d1 + d2 * d2 > C.dr2);
         if (TYPE == 5 && in) w.lj += (uint32_t)(C.a1 - C.a0);
+        fac[c] = in ? 1.0f : 0.0f;
       }
       const unsigned b = __ballot_sync(0xffffffffu, in);
       in_mask |= (unsigned long long)((b >> gbase) & gbits) << c0;
     }
+    if (lane == 0) fac[m.nc] = 0.0f;                   // the pad atoms' cluster
     Acc2 t = {};
     const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
     const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
@@ -412,12 +417,11 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         pair2j<TYPE>(m, j, f2(m.pl[j].z, m.pl[j].w), true, hx2, hy2, hz2, lx2, ly2, lz2, t);
       }
     } else {
+      ln.sync();
       for (int jb = 0; jb < (m.nslots >> 1); jb += G) {
         const int j = jb + lane;
         const uint2 c = m.pc[j];
-        const float2 e = f2(m.pl[j].z, m.pl[j].w);
-        const float2 eps = f2(((in_mask >> c.x) & 1ull) ? e.x : 0.0f,
-                              ((in_mask >> c.y) & 1ull) ? e.y : 0.0f);
+        const float2 eps = __fmul2_rn(f2(m.pl[j].z, m.pl[j].w), f2(fac[c.x], fac[c.y]));
         pair2j<TYPE>(m, j, eps, true, hx2, hy2, hz2, lx2, ly2, lz2, t);
       }
     }
