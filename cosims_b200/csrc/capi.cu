@@ -113,19 +113,6 @@ cosims_status validate(const cosims_molecule *mol, const cosims_params *par) {
   return COSIMS_OK;
 }
 
-// Whether the plain form's branch-free division and square root apply to the
-// molecule: every value that enters a dividend is zero or of magnitude in
-// [2^-400, 2^400] (the force loops check the position-dependent operands).
-int fast_arith_ok(const cosims_molecule *m) {
-  auto in = [](double v) {
-    const double a = std::fabs(v);
-    return a == 0.0 || (a >= 0x1p-400 && a <= 0x1p400);
-  };
-  for (int i = 0; i < m->n_atoms; i++)
-    if (!in(m->charge[i]) || !in(m->sig6[i]) || !in(m->eps24m[i]) || !in(m->eps4[i])) return 0;
-  return 1;
-}
-
 DevParams make_dev_params(const cosims_params *p) {
   DevParams d;
   std::memset(&d, 0, sizeof d);
@@ -602,14 +589,13 @@ cosims_status cosims_ctx_create(const cosims_molecule *mol, const cosims_params 
   c->sm_count = sm;
   c->max_smem = smem;
   c->par = make_dev_params(par);
-  c->par.fast_arith = fast_arith_ok(mol);
   c->n_atoms = mol->n_atoms;
   build_images(mol, par, c->h64, c->h32);
   c->img64 = c->h64.img;
   c->img32 = c->h32.img;
   c->group_lanes = precision == COSIMS_PRECISION_PLAIN_F64 ? 1 : default_group_lanes(mol->n_atoms);
   c->block_threads = precision == COSIMS_PRECISION_PLAIN_F64 ? 128 : 0;   // 0: chosen per run
-  if (precision == COSIMS_PRECISION_PLAIN_F64) c->ho_budget = kDefaultPlainHandoffBudget;
+  if (precision == COSIMS_PRECISION_PLAIN_F64) c->ho_budget = default_plain_budget(mol->n_atoms);
   cudaError_t e = cudaMalloc((void **)&c->d_img64, c->img64.bytes);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_img32, c->img32.bytes);
   if (e == cudaSuccess) e = cudaMalloc((void **)&c->d_queue, sizeof(unsigned long long));
@@ -689,7 +675,7 @@ cosims_status cosims_ctx_set_handoff(cosims_ctx *c, int64_t step_budget, int32_t
     return fail(COSIMS_ERR_INVALID, "the plain form's wide group is its %d-thread CTA", kPlainBlock);
   if (wide_lanes < 0 || wide_lanes > 512 || (wide_lanes & 31))
     return fail(COSIMS_ERR_INVALID, "wide_lanes must be 0 or a multiple of 32 up to 512");
-  const int64_t dflt = plain ? kDefaultPlainHandoffBudget : kDefaultHandoffBudget;
+  const int64_t dflt = plain ? default_plain_budget(c->n_atoms) : kDefaultHandoffBudget;
   c->ho_budget = step_budget == 0 ? dflt : (step_budget < 0 ? 0 : step_budget);
   c->ho_wide = wide_lanes;
   return COSIMS_OK;

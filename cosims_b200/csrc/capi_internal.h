@@ -23,7 +23,6 @@ cosims_status fail(cosims_status s, const char *fmt, ...);
 cosims_status cuda_fail(cudaError_t e, const char *what);
 cosims_status validate(const cosims_molecule *mol, const cosims_params *par);
 DevParams make_dev_params(const cosims_params *p);
-int fast_arith_ok(const cosims_molecule *m);
 void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h64,
                   HostImage &h32);
 int mode_stride_for(const MolImage &img, int force_type);

@@ -70,7 +70,10 @@ struct ClusterF64 {         // 176 bytes
   int32_t pad;
 };
 
-struct ClusterF32 {         // 112 bytes
+// 120 bytes: an odd number of 8-byte words, so that lanes reading consecutive
+// clusters' FP64 fields (the near/far pass, one cluster per lane) spread over
+// all shared-memory banks (a 112-byte stride put four lanes on each bank).
+struct ClusterF32 {
   double cx, cy, cz, mpr2, dr2;
   float q;
   float dip[3];
@@ -78,11 +81,12 @@ struct ClusterF32 {         // 112 bytes
   float qsig6, qeps;
   int32_t replaced;
   int32_t a0, a1;
+  int32_t pad[2];
 };
 
 static_assert(sizeof(AtomF64) == 56, "AtomF64 layout");
 static_assert(sizeof(ClusterF64) == 176, "ClusterF64 layout");
-static_assert(sizeof(ClusterF32) == 112, "ClusterF32 layout");
+static_assert(sizeof(ClusterF32) == 120, "ClusterF32 layout");
 
 struct MolImage {
   const unsigned char *gbase;   // image in global memory
@@ -106,11 +110,6 @@ struct DevParams {
   double b_max, start_dist, g_min, g_max, vdist_a, vdist_norm, vdist_max;
   double ccs_const;
   int64_t max_steps;
-  // plain form: the molecule's values allow the branch-free division and
-  // square root (every charge, sigma^6 and LJ prefactor zero or of magnitude
-  // in [2^-400, 2^400]); set by the host
-  int32_t fast_arith;
-  int32_t pad;
 };
 
 // Device-side counters of one run (all 64-bit, summed with atomics).
@@ -192,7 +191,14 @@ constexpr int kExactProducers = kPlainBlock - 32;
 constexpr int kExactPerThread = COSIMS_EXACT_PER_THREAD;
 constexpr int kExactChunk = kExactProducers * kExactPerThread;
 constexpr int kExactRow = kExactChunk + 1;
+// Plain form's default step budget: a CTA finishes a parked trajectory at
+// about 28x one thread's speed but with 128 threads, so the budget trades the
+// tail against wide-phase work.  Measured on B200 with calls of three 1e5
+// integrals: 256 is best for the 128-atom molecule, 1024 for the 512-atom ion.
 constexpr int64_t kDefaultPlainHandoffBudget = 256;
+inline int64_t default_plain_budget(int n_atoms) {
+  return n_atoms > 256 ? 1024 : kDefaultPlainHandoffBudget;
+}
 __host__ __device__ inline int exact_accumulators(int force_type) {
   return (force_type == 1 || force_type == 2) ? 15 : (force_type == 3 || force_type == 4) ? 12 : 4;
 }

@@ -130,8 +130,7 @@ extern "C" cosims_status cosims_run_list_noalloc(const cosims_molecule *mol,
   if (e != cudaSuccess) return cuda_fail(e, "no-alloc staging");
   if (n == 0) return COSIMS_OK;
 
-  DevParams dp = make_dev_params(par);
-  dp.fast_arith = fast_arith_ok(mol);
+  const DevParams dp = make_dev_params(par);
   int rc = order_launch(dp, d_vel0, nullptr, n, order, order_scratch, stream);
   if (rc != 0) return cuda_fail((cudaError_t)rc, "work-order launch");
 

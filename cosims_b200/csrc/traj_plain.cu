@@ -13,9 +13,7 @@
 // A thread whose trajectory ends takes the next one from a device work queue
 // at once, so a warp never waits on its slowest trajectory.
 #include <cuda_runtime.h>
-#include <type_traits>
 #include "device_util.cuh"
-#include "exact_arith.cuh"
 
 namespace cosims {
 namespace plain {
@@ -43,41 +41,12 @@ struct Work {          // per-thread work counters, flushed when a trajectory en
   uint32_t lj, es, pot, far;
 };
 
-// Division and square root of the force loops.  FAST: the branch-free
-// correctly rounded routines of exact_arith.cuh (bitwise IEEE inside their
-// range), with the squared distances that feed them checked against the range
-// (the caller redoes the evaluation with the IEEE operators when one is
-// outside); otherwise CUDA's IEEE operators.  Every division there has a
-// positive divisor built from a squared distance r2: r2 in [2^-100, 2^100]
-// keeps r2, r2^3 and r2^2 sqrt(r2) in [2^-300, 2^300], and the dividends
-// (1, sigma^6, charges, LJ prefactors -- the host checks the molecule's
-// values -- and their products with powers of r2) inside the dividend range.
-template <bool FAST>
-__device__ __forceinline__ double pdiv(double a, double b) {
-  if (FAST) return div_rn_pos(a, b);
-  return a / b;
-}
-template <bool FAST>
-__device__ __forceinline__ double psqrt(double x) {
-  if (FAST) return sqrt_rn(x);
-  return sqrt(x);
-}
-template <bool FAST>
-__device__ __forceinline__ bool r2_ok(double r2) {
-  if (!FAST) return true;
-  return (r2 >= 0x1p-100) & (r2 <= 0x1p100);
-}
-#define PDIV(a, b) pdiv<FAST>((a), (b))
-#define PSQRT(x) psqrt<FAST>((x))
-
 // multipoleCutoff (type 1, forceAccel.cpp:221-445) / multipoleOnly (type 2,
 // forceAccel.cpp:447-633): identical far-field block; in far clusters type 1
 // applies the dispersion cut-off with the parameters of atom index n (the
 // cluster index, forceAccel.cpp:353-355), type 2 uses each atom's own.
-template <bool FAST>
-__device__ bool force_multipole(const View &m, const DevParams &p, const double pos[3],
+__device__ void force_multipole(const View &m, const DevParams &p, const double pos[3],
                                 double acc[3], bool cutoff, Work &w) {
-  bool ok = true;
   double fieldX = 0, fieldY = 0, fieldZ = 0;
   double sMatXY = 0, sMatXZ = 0, sMatYZ = 0, aMatXY = 0, aMatXZ = 0, aMatYZ = 0;
   double diagMatXX = 0, diagMatYY = 0, diagMatZZ = 0;
@@ -90,12 +59,11 @@ __device__ bool force_multipole(const View &m, const DevParams &p, const double 
     const double multiPlusRad = m.cl[n].mpr2, dispPlusRad = m.cl[n].dr2;
     const int a0 = m.cl[n].a0, a1 = m.cl[n].a1;
     if (r2 > multiPlusRad) {
-      ok &= r2_ok<FAST>(r2);
       const double *D = m.cl[n].dip;
       const double *Q = m.cl[n].quad;
       const bool dipole = order >= 1 && !m.cl[n].replaced;
-      double r_2 = PDIV(1.0, r2);
-      double r_1 = PDIV(1.0, PSQRT(r2));
+      double r_2 = 1.0 / r2;
+      double r_1 = 1.0 / sqrt(r2);
       double r_3 = r_2 * r_1;
       double r_5 = r_3 * r_2;
       double r_7 = 0, const1 = 0, const2 = 0, t0 = 0, t1 = 0, t2 = 0;
@@ -156,11 +124,10 @@ __device__ bool force_multipole(const View &m, const DevParams &p, const double 
         for (int k = a0; k < a1; k++) {
           double ex0 = pos[0] - m.at[k].x, ex1 = pos[1] - m.at[k].y, ex2 = pos[2] - m.at[k].z;
           double rr2 = ex0 * ex0 + ex1 * ex1 + ex2 * ex2;
-          ok &= r2_ok<FAST>(rr2);
           double r6 = rr2 * rr2 * rr2;
-          double term2 = PDIV(cutoff ? s6 : m.at[k].sig6, r6);
+          double term2 = (cutoff ? s6 : m.at[k].sig6) / r6;
           double term1 = 2 * term2 * term2;
-          double scalarComp = PDIV((cutoff ? e24 : m.at[k].eps24m) * (term1 - term2), rr2);
+          double scalarComp = (cutoff ? e24 : m.at[k].eps24m) * (term1 - term2) / rr2;
           sumX += scalarComp * ex0;
           sumY += scalarComp * ex1;
           sumZ += scalarComp * ex2;
@@ -173,8 +140,7 @@ __device__ bool force_multipole(const View &m, const DevParams &p, const double 
         double charge = m.at[k].q;
         double ex0 = pos[0] - m.at[k].x, ex1 = pos[1] - m.at[k].y, ex2 = pos[2] - m.at[k].z;
         double rr2 = ex0 * ex0 + ex1 * ex1 + ex2 * ex2;
-        ok &= r2_ok<FAST>(rr2);
-        double r_5 = PDIV(1.0, rr2 * rr2 * PSQRT(rr2));
+        double r_5 = 1.0 / (rr2 * rr2 * sqrt(rr2));
         double r_3 = r_5 * rr2;
         r_3 *= charge;
         r_5 *= charge;
@@ -189,9 +155,9 @@ __device__ bool force_multipole(const View &m, const DevParams &p, const double 
         sMatYZ -= 3 * ex1 * ex2 * r_5;
         if (lj) {
           double r6 = rr2 * rr2 * rr2;
-          double term2 = PDIV(m.at[k].sig6, r6);
+          double term2 = m.at[k].sig6 / r6;
           double term1 = 2 * term2 * term2;
-          double scalarComp = PDIV(m.at[k].eps24m * (term1 - term2), rr2);
+          double scalarComp = m.at[k].eps24m * (term1 - term2) / rr2;
           sumX += scalarComp * ex0;
           sumY += scalarComp * ex1;
           sumZ += scalarComp * ex2;
@@ -205,14 +171,11 @@ __device__ bool force_multipole(const View &m, const DevParams &p, const double 
   sumY += ds * ((sMatXY - aMatXY) * fieldX + diagMatYY * fieldY + (sMatYZ + aMatYZ) * fieldZ);
   sumZ += ds * ((sMatXZ - aMatXZ) * fieldX + (sMatYZ - aMatYZ) * fieldY + diagMatZZ * fieldZ);
   acc[0] = sumX; acc[1] = sumY; acc[2] = sumZ;
-  return ok;
 }
 
 // dispersionOnly (type 3, forceAccel.cpp:635-749).
-template <bool FAST>
-__device__ bool force_dispersion_only(const View &m, const DevParams &p, const double pos[3],
+__device__ void force_dispersion_only(const View &m, const DevParams &p, const double pos[3],
                                       double acc[3], Work &w) {
-  bool ok = true;
   double fieldX = 0, fieldY = 0, fieldZ = 0;
   double sMatXY = 0, sMatXZ = 0, sMatYZ = 0;
   double diagMatXX = 0, diagMatYY = 0, diagMatZZ = 0;
@@ -227,8 +190,7 @@ __device__ bool force_dispersion_only(const View &m, const DevParams &p, const d
       double charge = m.at[k].q;
       double ex0 = pos[0] - m.at[k].x, ex1 = pos[1] - m.at[k].y, ex2 = pos[2] - m.at[k].z;
       double rr2 = ex0 * ex0 + ex1 * ex1 + ex2 * ex2;
-      ok &= r2_ok<FAST>(rr2);
-      double r_5 = PDIV(1.0, rr2 * rr2 * PSQRT(rr2));
+      double r_5 = 1.0 / (rr2 * rr2 * sqrt(rr2));
       double r_3 = r_5 * rr2;
       r_3 *= charge;
       r_5 *= charge;
@@ -243,9 +205,9 @@ __device__ bool force_dispersion_only(const View &m, const DevParams &p, const d
       sMatYZ -= 3 * ex1 * ex2 * r_5;
       if (lj) {
         double r6 = rr2 * rr2 * rr2;
-        double term2 = PDIV(m.at[k].sig6, r6);
+        double term2 = m.at[k].sig6 / r6;
         double term1 = 2 * term2 * term2;
-        double scalarComp = PDIV(m.at[k].eps24m * (term1 - term2), rr2);
+        double scalarComp = m.at[k].eps24m * (term1 - term2) / rr2;
         sumX += scalarComp * ex0;
         sumY += scalarComp * ex1;
         sumZ += scalarComp * ex2;
@@ -258,32 +220,28 @@ __device__ bool force_dispersion_only(const View &m, const DevParams &p, const d
   sumY += ds * (sMatXY * fieldX + diagMatYY * fieldY + sMatYZ * fieldZ);
   sumZ += ds * (sMatXZ * fieldX + sMatYZ * fieldY + diagMatZZ * fieldZ);
   acc[0] = sumX; acc[1] = sumY; acc[2] = sumZ;
-  return ok;
 }
 
 // chargeDipoleLJ (type 4, forceAccel.cpp:751-805).
-template <bool FAST>
-__device__ bool force_charge_dipole_lj(const View &m, const DevParams &p, const double pos[3],
+__device__ void force_charge_dipole_lj(const View &m, const DevParams &p, const double pos[3],
                                        double acc[3], Work &w) {
-  bool ok = true;
   double sumXX = 0, sumYY = 0, sumZZ = 0, sumXY = 0, sumXZ = 0, sumYZ = 0;
   double dipX = 0, dipY = 0, dipZ = 0, tempx = 0, tempy = 0, tempz = 0;
   for (int n = 0; n < m.n; n++) {
     double xDiff = pos[0] - m.at[n].x, yDiff = pos[1] - m.at[n].y, zDiff = pos[2] - m.at[n].z;
     double xDiff2 = xDiff * xDiff, yDiff2 = yDiff * yDiff, zDiff2 = zDiff * zDiff;
     double r2 = xDiff2 + yDiff2 + zDiff2;
-    ok &= r2_ok<FAST>(r2);
-    double r = PSQRT(r2);
+    double r = sqrt(r2);
     double r3 = r2 * r;
-    double r_3 = PDIV(1.0, r3);
-    double r_5 = PDIV(r_3, r2);
+    double r_3 = 1.0 / r3;
+    double r_5 = r_3 / r2;
     double r6 = r2 * r2 * r2;
     const double qn = m.at[n].q;
     r_3 *= qn;
     r_5 *= qn;
-    double term2 = PDIV(m.at[n].sig6, r6);
+    double term2 = m.at[n].sig6 / r6;
     double term1 = 2 * term2 * term2;
-    double scalarComp = PDIV(m.at[n].eps24m * (term1 - term2), r2);
+    double scalarComp = m.at[n].eps24m * (term1 - term2) / r2;
     tempx += scalarComp * xDiff;
     tempy += scalarComp * yDiff;
     tempz += scalarComp * zDiff;
@@ -303,14 +261,11 @@ __device__ bool force_charge_dipole_lj(const View &m, const DevParams &p, const 
   tempy -= ds * (sumXY * dipX + sumYY * dipY + sumYZ * dipZ);
   tempz -= ds * (sumXZ * dipX + sumYZ * dipY + sumZZ * dipZ);
   acc[0] = tempx; acc[1] = tempy; acc[2] = tempz;
-  return ok;
 }
 
 // dispersionNoCharge (type 5, forceAccel.cpp:807-854).
-template <bool FAST>
-__device__ bool force_dispersion_nocharge(const View &m, const double pos[3], double acc[3],
+__device__ void force_dispersion_nocharge(const View &m, const double pos[3], double acc[3],
                                           Work &w) {
-  bool ok = true;
   double sumX = 0, sumY = 0, sumZ = 0;
   for (int n = 0; n < m.nc; n++) {
     double dx0 = pos[0] - m.cl[n].cx, dx1 = pos[1] - m.cl[n].cy, dx2 = pos[2] - m.cl[n].cz;
@@ -321,11 +276,10 @@ __device__ bool force_dispersion_nocharge(const View &m, const double pos[3], do
       for (int k = a0; k < a1; k++) {
         double ex0 = pos[0] - m.at[k].x, ex1 = pos[1] - m.at[k].y, ex2 = pos[2] - m.at[k].z;
         double rr2 = ex0 * ex0 + ex1 * ex1 + ex2 * ex2;
-        ok &= r2_ok<FAST>(rr2);
         double r6 = rr2 * rr2 * rr2;
-        double term2 = PDIV(m.at[k].sig6, r6);
+        double term2 = m.at[k].sig6 / r6;
         double term1 = 2 * term2 * term2;
-        double scalarComp = PDIV(m.at[k].eps24m * (term1 - term2), rr2);
+        double scalarComp = m.at[k].eps24m * (term1 - term2) / rr2;
         sumX += scalarComp * ex0;
         sumY += scalarComp * ex1;
         sumZ += scalarComp * ex2;
@@ -334,76 +288,54 @@ __device__ bool force_dispersion_nocharge(const View &m, const double pos[3], do
     }
   }
   acc[0] = sumX; acc[1] = sumY; acc[2] = sumZ;
-  return ok;
 }
 
 // dispersionFull (type 6, forceAccel.cpp:856-884).
-template <bool FAST>
-__device__ bool force_dispersion_full(const View &m, const double pos[3], double acc[3],
+__device__ void force_dispersion_full(const View &m, const double pos[3], double acc[3],
                                       Work &w) {
-  bool ok = true;
   double tempx = 0, tempy = 0, tempz = 0;
   for (int n = 0; n < m.n; n++) {
     double xDiff = pos[0] - m.at[n].x, yDiff = pos[1] - m.at[n].y, zDiff = pos[2] - m.at[n].z;
     double xDiff2 = xDiff * xDiff, yDiff2 = yDiff * yDiff, zDiff2 = zDiff * zDiff;
     double r2 = xDiff2 + yDiff2 + zDiff2;
-    ok &= r2_ok<FAST>(r2);
     double r6 = r2 * r2 * r2;
-    double term2 = PDIV(m.at[n].sig6, r6);
+    double term2 = m.at[n].sig6 / r6;
     double term1 = 2 * term2 * term2;
-    double scalarComp = PDIV(m.at[n].eps24m * (term1 - term2), r2);
+    double scalarComp = m.at[n].eps24m * (term1 - term2) / r2;
     tempx += scalarComp * xDiff;
     tempy += scalarComp * yDiff;
     tempz += scalarComp * zDiff;
   }
   w.lj += m.n;
   acc[0] = tempx; acc[1] = tempy; acc[2] = tempz;
-  return ok;
 }
 
-template <int TYPE, bool FAST>
-__device__ __forceinline__ bool force_v(const View &m, const DevParams &p, const double pos[3],
-                                        double acc[3], Work &w) {
-  switch (TYPE) {
-    case 1: return force_multipole<FAST>(m, p, pos, acc, true, w);
-    case 2: return force_multipole<FAST>(m, p, pos, acc, false, w);
-    case 3: return force_dispersion_only<FAST>(m, p, pos, acc, w);
-    case 4: return force_charge_dipole_lj<FAST>(m, p, pos, acc, w);
-    case 5: return force_dispersion_nocharge<FAST>(m, pos, acc, w);
-    default: return force_dispersion_full<FAST>(m, pos, acc, w);
-  }
-}
-
-// The acceleration: the branch-free arithmetic when the molecule allows it
-// and every squared distance is in range, else the IEEE operators (the same
-// bits either way; the fallback only exists for out-of-range operands).
 template <int TYPE>
 __device__ __forceinline__ void force(const View &m, const DevParams &p, const double pos[3],
                                       double acc[3], Work &w) {
-  Work wf = w;
-  if (p.fast_arith && force_v<TYPE, true>(m, p, pos, acc, wf)) {
-    w = wf;
-    return;
+  switch (TYPE) {
+    case 1: force_multipole(m, p, pos, acc, true, w); break;
+    case 2: force_multipole(m, p, pos, acc, false, w); break;
+    case 3: force_dispersion_only(m, p, pos, acc, w); break;
+    case 4: force_charge_dipole_lj(m, p, pos, acc, w); break;
+    case 5: force_dispersion_nocharge(m, pos, acc, w); break;
+    default: force_dispersion_full(m, pos, acc, w); break;
   }
-  force_v<TYPE, false>(m, p, pos, acc, w);
 }
 
 // getPotential (forceAccel.cpp:943-982), atoms in file order.
-template <bool FAST>
-__device__ double potential_v(const View &m, const DevParams &p, const double pos[3], bool &ok) {
+__device__ double potential(const View &m, const DevParams &p, const double pos[3]) {
   double total = 0, sumX = 0, sumY = 0, sumZ = 0;
-  ok = true;
   for (int i = 0; i < m.n; i++) {
     const int k = m.uses_clusters ? m.perm[i] : i;
     double xDiff = pos[0] - m.at[k].x, yDiff = pos[1] - m.at[k].y, zDiff = pos[2] - m.at[k].z;
     double r2 = xDiff * xDiff + yDiff * yDiff + zDiff * zDiff;
-    ok &= r2_ok<FAST>(r2);
     double r6 = r2 * r2 * r2;
-    double term2 = PDIV(m.at[k].sig6, r6);
+    double term2 = m.at[k].sig6 / r6;
     double term1 = term2 * term2;
     total += m.at[k].eps4 * (term1 - term2);
     if (p.charged) {
-      double r_3 = PDIV(m.at[k].q, r2 * PSQRT(r2));
+      double r_3 = m.at[k].q / (r2 * sqrt(r2));
       sumX += xDiff * r_3;
       sumY += yDiff * r_3;
       sumZ += zDiff * r_3;
@@ -411,15 +343,6 @@ __device__ double potential_v(const View &m, const DevParams &p, const double po
   }
   if (p.charged) total -= p.dipole_scalar * 0.5 * (sumX * sumX + sumY * sumY + sumZ * sumZ);
   return total;
-}
-
-__device__ __forceinline__ double potential(const View &m, const DevParams &p, const double pos[3]) {
-  bool ok = false;
-  if (p.fast_arith) {
-    const double U = potential_v<true>(m, p, pos, ok);
-    if (ok) return U;
-  }
-  return potential_v<false>(m, p, pos, ok);
 }
 
 __device__ __forceinline__ double dot3(const double a[3], const double b[3]) {
@@ -525,8 +448,8 @@ __device__ __forceinline__ double exact_sum(const Exact &x, int nitems, int K, u
 
 // One event's terms for the force variants, as the serial loops of the
 // force_* functions above compute them.
-template <int TYPE, bool FAST>
-__device__ __forceinline__ bool event_terms(const View &m, const DevParams &p, const double pos[3],
+template <int TYPE>
+__device__ __forceinline__ void event_terms(const View &m, const DevParams &p, const double pos[3],
                                             const Exact &x, double *T, int j, int e, Work &w) {
   const int2 sl = m.slot[e];
   const Col o{T, j, sl.x < 0 ? -1 - sl.x : 0};
@@ -536,19 +459,18 @@ __device__ __forceinline__ bool event_terms(const View &m, const DevParams &p, c
     double xDiff = pos[0] - m.at[n].x, yDiff = pos[1] - m.at[n].y, zDiff = pos[2] - m.at[n].z;
     double xDiff2 = xDiff * xDiff, yDiff2 = yDiff * yDiff, zDiff2 = zDiff * zDiff;
     double r2 = xDiff2 + yDiff2 + zDiff2;
-    const bool ok = r2_ok<FAST>(r2);
     double r6 = r2 * r2 * r2;
-    double term2 = PDIV(m.at[n].sig6, r6);
+    double term2 = m.at[n].sig6 / r6;
     double term1 = 2 * term2 * term2;
-    double scalarComp = PDIV(m.at[n].eps24m * (term1 - term2), r2);
+    double scalarComp = m.at[n].eps24m * (term1 - term2) / r2;
     o.put(0, 0, scalarComp * xDiff);
     o.put(1, 0, scalarComp * yDiff);
     o.put(2, 0, scalarComp * zDiff);
     if (type == 4) {
-      double r = PSQRT(r2);
+      double r = sqrt(r2);
       double r3 = r2 * r;
-      double r_3 = PDIV(1.0, r3);
-      double r_5 = PDIV(r_3, r2);
+      double r_3 = 1.0 / r3;
+      double r_5 = r_3 / r2;
       const double qn = m.at[n].q;
       r_3 *= qn;
       r_5 *= qn;
@@ -565,44 +487,42 @@ __device__ __forceinline__ bool event_terms(const View &m, const DevParams &p, c
     } else {
       w.lj++;
     }
-    return ok;
+    return;
   }
   const int c = sl.y;
   const uint8_t flag = x.cflag[c];
   const bool far = flag & 1u, in_lj = (flag & 2u) != 0;
   if (type == 5) {
-    if (!in_lj) return true;
+    if (!in_lj) return;
     const int k = sl.x;
     double ex0 = pos[0] - m.at[k].x, ex1 = pos[1] - m.at[k].y, ex2 = pos[2] - m.at[k].z;
     double rr2 = ex0 * ex0 + ex1 * ex1 + ex2 * ex2;
-    const bool ok = r2_ok<FAST>(rr2);
     double r6 = rr2 * rr2 * rr2;
-    double term2 = PDIV(m.at[k].sig6, r6);
+    double term2 = m.at[k].sig6 / r6;
     double term1 = 2 * term2 * term2;
-    double scalarComp = PDIV(m.at[k].eps24m * (term1 - term2), rr2);
+    double scalarComp = m.at[k].eps24m * (term1 - term2) / rr2;
     o.put(0, 0, scalarComp * ex0);
     o.put(1, 0, scalarComp * ex1);
     o.put(2, 0, scalarComp * ex2);
     w.lj++;
-    return ok;
+    return;
   }
   // variants 1, 2, 3: accumulators fieldXYZ 0-2, diagMat 3-5, sMat 6-8 (minus),
   // aMat 9-11 (variants 1, 2), LJ sums 9-11 (variant 3) or 12-14 (1, 2)
   const bool cutoff = type == 1;
   const int ljk = type == 3 ? 9 : 12;
   if (sl.x < 0) {                       // far field of cluster c (variants 1, 2)
-    if (!far) return true;
+    if (!far) return;
     const ClusterF64 &C = m.cl[c];
     double dx0 = pos[0] - C.cx, dx1 = pos[1] - C.cy, dx2 = pos[2] - C.cz;
     double xx = dx0 * dx0, yy = dx1 * dx1, zz = dx2 * dx2;
     double r2 = xx + yy + zz;
-    const bool ok = r2_ok<FAST>(r2);
     const double *D = C.dip;
     const double *Q = C.quad;
     const int order = p.multipole_order;
     const bool dipole = order >= 1 && !C.replaced;
-    double r_2 = PDIV(1.0, r2);
-    double r_1 = PDIV(1.0, PSQRT(r2));
+    double r_2 = 1.0 / r2;
+    double r_1 = 1.0 / sqrt(r2);
     double r_3 = r_2 * r_1;
     double r_5 = r_3 * r_2;
     double r_7 = 0, const1 = 0, const2 = 0, t0 = 0, t1 = 0, t2 = 0;
@@ -661,33 +581,31 @@ __device__ __forceinline__ bool event_terms(const View &m, const DevParams &p, c
       o.put(11, pa, 5 * (t2 * dx1 - t1 * dx2));
     }
     if (o.part == 0) w.far++;
-    return ok;
+    return;
   }
   const int k = sl.x;
   if (type != 3 && far) {               // far cluster: the LJ band only
-    if (cutoff && !in_lj) return true;
+    if (cutoff && !in_lj) return;
     const ClusterF64 &C = m.cl[c];
     const double s6 = cutoff ? C.qsig6 : 0.0, e24 = cutoff ? C.qeps : 0.0;
     double ex0 = pos[0] - m.at[k].x, ex1 = pos[1] - m.at[k].y, ex2 = pos[2] - m.at[k].z;
     double rr2 = ex0 * ex0 + ex1 * ex1 + ex2 * ex2;
-    const bool ok = r2_ok<FAST>(rr2);
     double r6 = rr2 * rr2 * rr2;
-    double term2 = PDIV(cutoff ? s6 : m.at[k].sig6, r6);
+    double term2 = (cutoff ? s6 : m.at[k].sig6) / r6;
     double term1 = 2 * term2 * term2;
-    double scalarComp = PDIV((cutoff ? e24 : m.at[k].eps24m) * (term1 - term2), rr2);
+    double scalarComp = (cutoff ? e24 : m.at[k].eps24m) * (term1 - term2) / rr2;
     o.put(ljk, 0, scalarComp * ex0);
     o.put(ljk + 1, 0, scalarComp * ex1);
     o.put(ljk + 2, 0, scalarComp * ex2);
     w.lj++;
-    return ok;
+    return;
   }
   // a near cluster (or any cluster of variant 3): charge field, and LJ inside the cut-off
   const bool lj = type == 2 || in_lj;
   double charge = m.at[k].q;
   double ex0 = pos[0] - m.at[k].x, ex1 = pos[1] - m.at[k].y, ex2 = pos[2] - m.at[k].z;
   double rr2 = ex0 * ex0 + ex1 * ex1 + ex2 * ex2;
-  const bool ok = r2_ok<FAST>(rr2);
-  double r_5 = PDIV(1.0, rr2 * rr2 * PSQRT(rr2));
+  double r_5 = 1.0 / (rr2 * rr2 * sqrt(rr2));
   double r_3 = r_5 * rr2;
   r_3 *= charge;
   r_5 *= charge;
@@ -702,15 +620,14 @@ __device__ __forceinline__ bool event_terms(const View &m, const DevParams &p, c
   o.put(8, 0, 3 * ex1 * ex2 * r_5);
   if (lj) {
     double r6 = rr2 * rr2 * rr2;
-    double term2 = PDIV(m.at[k].sig6, r6);
+    double term2 = m.at[k].sig6 / r6;
     double term1 = 2 * term2 * term2;
-    double scalarComp = PDIV(m.at[k].eps24m * (term1 - term2), rr2);
+    double scalarComp = m.at[k].eps24m * (term1 - term2) / rr2;
     o.put(ljk, 0, scalarComp * ex0);
     o.put(ljk + 1, 0, scalarComp * ex1);
     o.put(ljk + 2, 0, scalarComp * ex2);
   }
   w.es++;
-  return ok;
 }
 
 // The acceleration of the serial force functions, by the whole CTA.
@@ -730,12 +647,7 @@ __device__ void exact_force(const View &m, const DevParams &p, const double pos[
   // sMat (accumulators 6-8) is decremented by variants 1, 2 and 3
   const uint32_t minus = (type == 1 || type == 2 || type == 3) ? 0x1c0u : 0u;
   const double a = exact_sum(x, m.nslot, x.K, minus, [&](double *T, int j, int e) {
-    Work wf = w;
-    if (p.fast_arith && event_terms<TYPE, true>(m, p, pos, x, T, j, e, wf)) {
-      w = wf;
-      return;
-    }
-    event_terms<TYPE, false>(m, p, pos, x, T, j, e, w);
+    event_terms<TYPE>(m, p, pos, x, T, j, e, w);
   });
   if (threadIdx.x < x.K) x.accs[threadIdx.x] = a;
   __syncthreads();
@@ -769,29 +681,21 @@ __device__ void exact_force(const View &m, const DevParams &p, const double pos[
 __device__ double exact_potential(const View &m, const DevParams &p, const double pos[3],
                                   const Exact &x, Work &w) {
   const int K = p.charged ? 4 : 1;
-  // one atom's terms; FAST as in the force loops (false: IEEE operators)
-  auto terms = [&](auto fast, double *T, int j, int i) -> bool {
-    constexpr bool FAST = decltype(fast)::value;
+  const double a = exact_sum(x, m.n, K, 0u, [&](double *T, int j, int i) {
     const Col o{T, j, 0};
     const int k = m.uses_clusters ? m.perm[i] : i;
     double xDiff = pos[0] - m.at[k].x, yDiff = pos[1] - m.at[k].y, zDiff = pos[2] - m.at[k].z;
     double r2 = xDiff * xDiff + yDiff * yDiff + zDiff * zDiff;
-    const bool ok = r2_ok<FAST>(r2);
     double r6 = r2 * r2 * r2;
-    double term2 = PDIV(m.at[k].sig6, r6);
+    double term2 = m.at[k].sig6 / r6;
     double term1 = term2 * term2;
     o.put(0, 0, m.at[k].eps4 * (term1 - term2));
     if (p.charged) {
-      double r_3 = PDIV(m.at[k].q, r2 * PSQRT(r2));
+      double r_3 = m.at[k].q / (r2 * sqrt(r2));
       o.put(1, 0, xDiff * r_3);
       o.put(2, 0, yDiff * r_3);
       o.put(3, 0, zDiff * r_3);
     }
-    return ok;
-  };
-  const double a = exact_sum(x, m.n, K, 0u, [&](double *T, int j, int i) {
-    if (p.fast_arith && terms(std::true_type{}, T, j, i)) return;
-    terms(std::false_type{}, T, j, i);
   });
   if (threadIdx.x < K) x.accs[threadIdx.x] = a;
   __syncthreads();

@@ -85,8 +85,6 @@ def lib():
                 "cosims_serve_release": (st, [V, C.c_int64]),
                 "cosims_serve_info": (st, [V, P(C.c_int32), P(C.c_int64)]),
                 "cosims_probe_peaks": (st, [C.c_int32, P(C.c_double), P(C.c_double)]),
-                "cosims_check_exact_arith": (st, [C.c_int32, C.c_uint64, C.c_int64,
-                                                  P(C.c_int64), P(C.c_int64)]),
             }
             for name, (res, args) in sig.items():
                 f = getattr(L, name)
@@ -417,10 +415,3 @@ def omega(s: abi.CcsSums) -> tuple:
     var = s.sum2 / n - m * m
     return m, float(np.sqrt(max(var, 0.0) / n))
 
-
-def check_exact_arith(device: int = 0, seed: int = 1, n: int = 1 << 24) -> tuple:
-    """Results of the plain form's branch-free division and square root that
-    differ from CUDA's IEEE operators on n operand pairs: (div, sqrt)."""
-    d, q = C.c_int64(), C.c_int64()
-    check(lib().cosims_check_exact_arith(device, seed, n, C.byref(d), C.byref(q)))
-    return d.value, q.value

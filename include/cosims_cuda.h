@@ -196,7 +196,7 @@ cosims_status cosims_ctx_get_launch(const cosims_ctx *ctx, int32_t *group_lanes,
  * Plain form: the wide group is the whole 128-thread CTA (wide_lanes 0 or
  * 128), which evaluates a step's terms in parallel and adds them in the
  * reference's order: results are bitwise those without hand-off, whatever
- * the budget.  Default step_budget 256.
+ * the budget.  Default step_budget 256 up to 256 atoms, 1024 above.
  * step_budget: 0 = default, < 0 = off.  The context keeps a 200-byte record
  * per trajectory of a call for this; calls of more than 2^22 trajectories run
  * without hand-off. */
@@ -307,16 +307,6 @@ cosims_status cosims_ctx_kernel_timeline(cosims_ctx *ctx, double *drain_ms, doub
  * reference: the roofline denominator for the trajectory kernels, which are
  * bound by these pipes rather than by HBM or the tensor cores. */
 cosims_status cosims_probe_peaks(int32_t device, double *fp32_tflops, double *fp64_tflops);
-
-/* Self-check of the branch-free FP64 division and square root that the plain
- * form's force loops use in place of the IEEE operators (whose slow-path
- * branches serialise the per-atom dependency chains): n operand pairs per
- * call, drawn from `seed`, over the whole valid range, the force loops'
- * physical ranges and mantissa edge cases; div_mismatches / sqrt_mismatches
- * receive the results that differ from CUDA's `/` and `sqrt` in any bit (0
- * expected).  No counterpart in the reference. */
-cosims_status cosims_check_exact_arith(int32_t device, uint64_t seed, int64_t n,
-                                       int64_t *div_mismatches, int64_t *sqrt_mismatches);
 
 /* ---- no device allocation ------------------------------------------------ */
 /* No counterpart in the reference.  For callers that cannot let this library

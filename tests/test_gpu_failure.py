@@ -20,7 +20,8 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("precision", [abi.PLAIN_F64, abi.MIXED])
 def test_staging_wait_gives_up_and_context_recovers(precision):
-    mol, par, d = load("c1_t3")
+    # the 128-atom molecule: both forms stage its image in shared memory
+    mol, par, d = load("c0_t5")
     p0, v0 = hits(d)
     with engine.Context(mol, par, precision) as ctx:
         good = ctx.run_list(p0, v0)
@@ -63,9 +64,10 @@ def test_wait_test_rejects_unknown_flags():
 
 
 def test_energy_check_fails_every_retry_like_the_reference():
-    """dt = 0.5 ps (50x the default) cannot keep the energy within 0.5 %: the
-    trajectories fail after their energy retries with chi = pi/2, exactly as
-    the oracle's verletVel restatement says, retry counts included."""
+    """dt = 0.5 ps (50x the default) cannot keep the energy within 0.5 % on
+    close collisions: those trajectories fail after their energy retries with
+    chi = pi/2, exactly as the oracle's verletVel restatement says, retry
+    counts included."""
     mol, par, d = load("q128_t3")
     p0, v0 = hits(d)
     p0, v0 = p0[:64], v0[:64]
@@ -77,7 +79,7 @@ def test_energy_check_fails_every_retry_like_the_reference():
     np.testing.assert_array_equal(out["steps"], ref["steps"])
     assert np.max(np.abs(out["chi"] - ref["chi"])) <= 1e-12
     failed = (out["status"] & abi.TRAJ_SUCCESS) == 0
-    assert failed.mean() > 0.5
+    assert failed.sum() >= 4
     assert np.all(out["chi"][failed] == np.pi / 2)
     etries = (out["status"] >> abi.TRAJ_ETRIES_SHIFT) & 0xff
     assert etries[failed].max() >= 1
