@@ -246,8 +246,13 @@ def profile_case(args, mol, par, stream, torch) -> None:
         if args.profile_budget:
             ctx.set_handoff(args.profile_budget, 0)
         n = args.profile_traj
+        m = max(1, args.profile_integrals)
+        d_many = torch.zeros((m + 1) * 128, dtype=torch.uint8, device="cuda")
         for k in range(args.warmup + args.steps):
-            ctx.run_sampled_device(SEED, k * n, n, 0, d_sums.data_ptr(), stream)
+            if m == 1:
+                ctx.run_sampled_device(SEED, k * n, n, 0, d_sums.data_ptr(), stream)
+            else:               # m integrals in one launch, as the timed call runs them
+                ctx.run_integrals_device(SEED, k * m * n, n, m, 0, d_many.data_ptr(), 0, stream)
             ms = ctx.kernel_ms()
         torch.cuda.synchronize()
         print(json.dumps({"profile": args.profile, "traj": n, "launch": ctx.get_launch(),
@@ -545,6 +550,8 @@ def serving_block(args, local, torch, library=None, duration: float | None = Non
     srv.close()
     lat = np.array([d_["latency"] for d_ in done])
     lat_setup = np.array([d_["latency"] + per_setup[d_["mol"]] for d_ in done])
+    tgt = np.array([d_["target"] for d_ in done])
+    ntraj = np.array([d_["n"] for d_ in done])
     # 5 % of the requests against the plain FP64 form on the same trajectories
     sample = done[::20]
     errs = []
@@ -570,6 +577,12 @@ def serving_block(args, local, torch, library=None, duration: float | None = Non
         "value": traj_done / wall, "unit": UNIT,
         "latency_s": {"p50": pct(lat, 50), "p99": pct(lat, 99), "max": pct(lat, 100)},
         "latency_with_setup_s": {"p50": pct(lat_setup, 50), "p99": pct(lat_setup, 99)},
+        "latency_by_target_s": {
+            f"{t * 100:g}%": {"requests": int(np.sum(tgt == t)),
+                              "p50": pct(lat[tgt == t], 50), "p99": pct(lat[tgt == t], 99),
+                              "traj_mean": float(ntraj[tgt == t].mean()) if np.any(tgt == t)
+                              else None}
+            for t in (0.005, 0.002)},
         "host_setup_s_per_molecule": {"mean": setup_s / len(lib_),
                                       "max": float(np.max(per_setup))},
         "ccs_err_pct_vs_plain_f64": {"max": max(errs) if errs else None,
@@ -739,6 +752,8 @@ def main():
                     help="hand-off step budget of the profiled run (0: the default; < 0: off)")
     ap.add_argument("--profile-max-steps", type=int, default=0,
                     help="step cap of the profiled run's trajectories (0: the default)")
+    ap.add_argument("--profile-integrals", type=int, default=1,
+                    help="integrals of --profile-traj trajectories per launch of the profiled run")
     ap.add_argument("--profile-config", type=int, default=1, choices=[0, 1, 2],
                     help="molecule of the profiled run: 0 the 128-atom neutral molecule, "
                          "1 the 512-atom ion (default), 2 the 3000-atom protein")
