@@ -70,3 +70,58 @@ def test_two_gloo_ranks_merge_like_one_place():
     assert merged["omega"] == pytest.approx(tot_sum / tot_n, rel=1e-15)
     assert slowest == 11.0
     assert shard.first_index(1) - shard.first_index(0) == shard.RANK_SPAN
+
+
+def _inputs(rank: int, n: int, par) -> np.ndarray:
+    """Sampled start values of rank `rank`'s trajectory range: each trajectory's
+    values are a function of its global index only (as the device sampler's
+    counter-based stream), drawn with the reference's distributions."""
+    out = np.zeros(n, abi.TRAJ_IN_DTYPE)
+    first = shard.first_index(rank)
+    for i in range(n):
+        rng = np.random.Generator(np.random.PCG64(first + i))
+        u = rng.random(5)
+        out[i] = (par.b_max * math.sqrt(u[0]), 2 * math.pi * u[1], math.acos(1 - 2 * u[2]),
+                  2 * math.pi * u[3], par.g_min + (par.g_max - par.g_min) * u[4])
+    return out
+
+
+def _integrating_worker(rank, world, port, n, q):
+    from tests.common import load
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    mol, par, _ = load("c0_t5")
+    out = oracle.run_inputs(mol, par, _inputs(rank, n, par))   # this rank's trajectories
+    s = oracle.reduce(par, out, 0)
+    merged = shard.merge_sums([s], dist, "cpu")
+    if rank == 0:
+        q.put(merged)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_integrating_their_ranges_merge_like_one_place():
+    """Each rank integrates its own trajectory range (the oracle's verletVel
+    restatement stands in for the GPU on CPU ranks); the merged CCS equals the
+    same ranges integrated and reduced in one process."""
+    from tests.common import load
+    world, n = 2, 24
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_integrating_worker, args=(r, world, port, n, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    merged = q.get(timeout=300)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    mol, par, _ = load("c0_t5")
+    ref = [oracle.reduce(par, oracle.run_inputs(mol, par, _inputs(r, n, par)), 0)
+           for r in range(world)]
+    assert merged["sum"] == sum(s.sum for s in ref)
+    assert merged["sum2"] == sum(s.sum2 for s in ref)
+    assert merged["n_eff"] == sum(s.n_eff for s in ref) and merged["n"] == world * n
+    assert merged["n_hit"] == sum(s.n_hit for s in ref) > 0
