@@ -193,11 +193,12 @@ constexpr int kExactChunk = kExactProducers * kExactPerThread;
 constexpr int kExactRow = kExactChunk + 1;
 // Plain form's default step budget: a CTA finishes a parked trajectory at
 // about 28x one thread's speed but with 128 threads, so the budget trades the
-// tail against wide-phase work.  Measured on B200 with calls of three 1e5
-// integrals: 256 is best for the 128-atom molecule, 1024 for the 512-atom ion.
+// tail against wide-phase work.  Measured on B200 (single integrals and calls
+// of three): 256 is best for the 128-atom molecule, 512 for the 512-atom ion
+// and the 3000-atom protein.
 constexpr int64_t kDefaultPlainHandoffBudget = 256;
 inline int64_t default_plain_budget(int n_atoms) {
-  return n_atoms > 256 ? 1024 : kDefaultPlainHandoffBudget;
+  return n_atoms > 256 ? 512 : kDefaultPlainHandoffBudget;
 }
 __host__ __device__ inline int exact_accumulators(int force_type) {
   return (force_type == 1 || force_type == 2) ? 15 : (force_type == 3 || force_type == 4) ? 12 : 4;

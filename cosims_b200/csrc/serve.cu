@@ -42,7 +42,7 @@ namespace {
 
 constexpr int kServeBlock = kBatchMaxBlock;
 constexpr uint32_t kServeImageCap = 96 * 1024;
-constexpr int64_t kMaxChunkRounds = 16;   // a chunk is at most 16 round_traj
+constexpr int64_t kMaxChunkRounds = 16;   // default: a chunk is at most 16 round_traj
 constexpr int kRounds = 3;                // rounds in flight at most
 constexpr size_t kArenaAlign = 256;
 constexpr size_t kStageBytes = size_t(8) << 20;   // pinned staging of job images
@@ -119,6 +119,7 @@ using namespace cosims;
 struct cosims_server {
   int device = 0, sm_count = 0, max_smem = 0;
   int64_t budget = 0, in_use = 0, round_traj = 0, next_id = 1;
+  int64_t max_chunk = 0;                     // trajectories of one job in one round, at most
   int32_t max_jobs = 0;
   int items_cap = 0;
   std::map<int64_t, Job> jobs;
@@ -233,7 +234,7 @@ cosims_status harvest(cosims_server *s, int r, int *finished) {
         want = (int64_t)std::ceil(std::max(need, 0.0) / (double)s->round_traj) * s->round_traj;
       }
       want = std::max<int64_t>(want, j.min_traj - j.done);
-      const int64_t cap = std::min<int64_t>(kMaxChunkRounds * s->round_traj, pool);
+      const int64_t cap = std::min<int64_t>(s->max_chunk, pool);
       j.next_chunk = std::min<int64_t>(std::max<int64_t>(want, s->round_traj), cap);
     } else {
       j.state = COSIMS_JOB_DONE;
@@ -402,6 +403,7 @@ cosims_status cosims_serve_create(int32_t device, int64_t hbm_budget_bytes, int3
   s->budget = hbm_budget_bytes;
   s->max_jobs = max_jobs;
   s->round_traj = round_traj;
+  s->max_chunk = kMaxChunkRounds * round_traj;
   // at most three items per CTA of two resident CTAs per SM, plus one per job
   s->items_cap = 3 * 2 * sm + max_jobs + 64;
   const int64_t slots = (int64_t)max_jobs * round_traj;
@@ -504,7 +506,7 @@ cosims_status cosims_serve_submit(cosims_server *s, const cosims_molecule *mol,
   j.n_atoms = mol->n_atoms;
   j.footprint = fp;
   j.arena_off = off;
-  j.next_chunk = std::max<int64_t>(s->round_traj, std::min<int64_t>(min_traj, kMaxChunkRounds * s->round_traj));
+  j.next_chunk = std::max<int64_t>(s->round_traj, std::min<int64_t>(min_traj, s->max_chunk));
   j.next_chunk = std::min<int64_t>(j.next_chunk, (int64_t)s->max_jobs * s->round_traj);
   BatchMol &bm = j.bm;
   std::memset(&bm, 0, sizeof bm);
@@ -607,6 +609,14 @@ cosims_status cosims_serve_release(cosims_server *s, int64_t job_id) {
   s->in_use -= j.footprint;
   s->free_slots.push_back(j.slot);
   s->jobs.erase(it);
+  return COSIMS_OK;
+}
+
+cosims_status cosims_serve_set_max_chunk(cosims_server *s, int64_t max_chunk_traj) {
+  if (!s) return fail(COSIMS_ERR_INVALID, "server is NULL");
+  if (max_chunk_traj < 0) return fail(COSIMS_ERR_INVALID, "max_chunk_traj must be >= 0");
+  s->max_chunk = max_chunk_traj == 0 ? kMaxChunkRounds * s->round_traj
+                                     : std::max<int64_t>(max_chunk_traj, s->round_traj);
   return COSIMS_OK;
 }
 

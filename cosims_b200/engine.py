@@ -84,6 +84,7 @@ def lib():
                 "cosims_serve_poll": (st, [V, C.c_int64, P(abi.JobStatus)]),
                 "cosims_serve_release": (st, [V, C.c_int64]),
                 "cosims_serve_info": (st, [V, P(C.c_int32), P(C.c_int64)]),
+                "cosims_serve_set_max_chunk": (st, [V, C.c_int64]),
                 "cosims_probe_peaks": (st, [C.c_int32, P(C.c_double), P(C.c_double)]),
             }
             for name, (res, args) in sig.items():
@@ -392,6 +393,10 @@ class Server:
 
     def release(self, job_id: int) -> None:
         check(lib().cosims_serve_release(self._h, job_id))
+
+    def set_max_chunk(self, max_chunk_traj: int) -> None:
+        """Largest chunk of one job in one round (0: the default, 16 round_traj)."""
+        check(lib().cosims_serve_set_max_chunk(self._h, int(max_chunk_traj)))
 
     def info(self) -> tuple:
         a, b = C.c_int32(), C.c_int64()

@@ -196,7 +196,7 @@ cosims_status cosims_ctx_get_launch(const cosims_ctx *ctx, int32_t *group_lanes,
  * Plain form: the wide group is the whole 128-thread CTA (wide_lanes 0 or
  * 128), which evaluates a step's terms in parallel and adds them in the
  * reference's order: results are bitwise those without hand-off, whatever
- * the budget.  Default step_budget 256 up to 256 atoms, 1024 above.
+ * the budget.  Default step_budget 256 up to 256 atoms, 512 above.
  * step_budget: 0 = default, < 0 = off.  The context keeps a 200-byte record
  * per trajectory of a call for this; calls of more than 2^22 trajectories run
  * without hand-off. */
@@ -427,6 +427,11 @@ cosims_status cosims_serve_poll(cosims_server *s, int64_t job_id, cosims_job_sta
 /* Frees a job's device resources (its slot and footprint return to the pool). */
 cosims_status cosims_serve_release(cosims_server *s, int64_t job_id);
 cosims_status cosims_serve_info(const cosims_server *s, int32_t *active, int64_t *bytes_in_use);
+/* The most trajectories one job integrates in one round (0: the default, 16
+ * round_traj; at least round_traj).  Larger chunks let jobs that need many
+ * trajectories finish in fewer rounds, at the cost of longer rounds for the
+ * jobs that share them.  Applies to chunks sized after this call. */
+cosims_status cosims_serve_set_max_chunk(cosims_server *s, int64_t max_chunk_traj);
 
 #ifdef __cplusplus
 }
