@@ -212,8 +212,8 @@ def autotune(ctx, stream, torch, d_sums) -> int:
     return best
 
 
-def timed_integrals(ctx, first: int, k: int, stream, torch, flush):
-    """k CCS integrals of N_TRAJ trajectories through cosims_run_integrals_device
+def timed_integrals(ctx, first: int, k: int, stream, torch, flush, n: int = N_TRAJ):
+    """k CCS integrals of n trajectories through cosims_run_integrals_device
     (one call, device-resident records), timed on the stream with CUDA events.
     Returns (ms of the call, per-integral sums, work record)."""
     from cosims_b200 import abi
@@ -222,8 +222,7 @@ def timed_integrals(ctx, first: int, k: int, stream, torch, flush):
     flush.zero_()                                   # L2 flush before the call
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(stream)
-    ctx.run_integrals_device(SEED, first, N_TRAJ, k, 0, d.data_ptr(), d.data_ptr() + k * sz,
-                             stream)
+    ctx.run_integrals_device(SEED, first, n, k, 0, d.data_ptr(), d.data_ptr() + k * sz, stream)
     b.record(stream)
     torch.cuda.synchronize()
     raw = d.cpu().numpy()
@@ -504,8 +503,8 @@ def serving_block(args, local, torch, library=None, duration: float | None = Non
     molecule of the configuration-3 library and a target relative standard
     error (0.5 %, or 0.2 % for one request in ten).  Requests are admitted as
     slots and HBM budget free up, run in rounds with everything else in
-    flight, and retire at their target.  The offered rate is 80 % of the
-    capacity measured on a burst of requests first (the configuration's
+    flight, and retire at their target.  The offered rate is 75 % of the
+    capacity measured on a burst of 96 requests first (the configuration's
     50 req/s exceeds one B200's capacity for this mix).  Latency is from
     arrival to retirement; the per-molecule host setup is reported apart and
     as a second latency figure with each request's own setup time added."""
@@ -534,11 +533,11 @@ def serving_block(args, local, torch, library=None, duration: float | None = Non
         return which, target
 
     # capacity: a burst of requests all present at t = 0
-    n_burst = 48
+    n_burst = 96
     w_b, t_b = draw(n_burst)
     done_b, wall_b, _ = serve_stream(srv, lib_, np.zeros(n_burst), w_b, t_b, 10 ** 6, round_traj)
     capacity = len(done_b) / wall_b
-    rate = args.rate if args.rate > 0 else 0.8 * capacity
+    rate = args.rate if args.rate > 0 else 0.75 * capacity
     n_req = int(rate * duration * 1.5) + 16
     arrivals = np.cumsum(rng.exponential(1.0 / rate, size=n_req))
     arrivals = arrivals[arrivals < duration]
@@ -567,7 +566,7 @@ def serving_block(args, local, torch, library=None, duration: float | None = Non
         errs.append(abs(r["omega"] - om) / om * 100.0)
     pct = lambda a, q: float(np.percentile(a, q)) if len(a) else None
     return {
-        "workload": f"serving: Poisson arrivals for {duration:g} s at 80 % of the measured "
+        "workload": f"serving: Poisson arrivals for {duration:g} s at 75 % of the measured "
                     f"capacity; molecules from a {len(lib_)}-molecule configuration-3 library; "
                     "target rel. SE 0.5 % (0.2 % for 10 %)",
         "capacity_req_per_s": capacity, "offered_req_per_s": rate,
@@ -619,7 +618,9 @@ def molecule_workload(args, rank, world, local, dist, torch):
     one step = one integral of 1e6 trajectories in the mixed form; the CCS
     error against the plain FP64 form is taken on the first 1e4 of them.
     small (configuration 0): neutral 128-atom molecule (variant 5); one step =
-    one integral of 1e4 trajectories in the plain FP64 form (the drop-in)."""
+    one integral of 1e4 trajectories in the plain FP64 form (the drop-in).
+    The K timed integrals (and the W warm-up ones) are one cosims_run_integrals
+    call each, as in the default line."""
     import numpy as np
     from cosims_b200 import abi, engine, host, shard, synth
     protein = args.workload == "protein"
@@ -634,7 +635,6 @@ def molecule_workload(args, rank, world, local, dist, torch):
     stream = torch.cuda.current_stream()
     d = torch.zeros(1024, dtype=torch.uint8, device="cuda")
     sz = abi.C.sizeof(abi.CcsSums)
-    step_sums = torch.zeros((args.steps, 128), dtype=torch.uint8, device="cuda")
     flush = torch.empty(512 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     first0 = shard.first_index(rank)
     ctx = engine.Context(mol, par, form, device=local)
@@ -647,37 +647,24 @@ def molecule_workload(args, rank, world, local, dist, torch):
             best = min(best, (ctx.kernel_ms(), lanes))
         g = best[1]
         ctx.set_launch(group_lanes=g)
-    for w in range(args.warmup):
-        ctx.run_sampled_device(SEED, first0 + w * n_traj, n_traj, 0, d.data_ptr(), stream)
-    torch.cuda.synchronize()
+    # warm-up and timed integrals each through one cosims_run_integrals call
+    timed_integrals(ctx, first0, args.warmup, stream, torch, flush, n_traj)
     clocks = ClockSampler(local)
     clocks.start()
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    ms, kern = [], []
-    for k in range(args.steps):
-        flush.zero_()
-        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        ctx.run_sampled_device(SEED, first0 + (args.warmup + k) * n_traj, n_traj, 0,
-                               step_sums[k].data_ptr(), stream)
-        e.record(stream)
-        torch.cuda.synchronize()
-        ms.append(a.elapsed_time(e))
-        kern.append(ctx.kernel_ms())
+    call_ms, sums, work = timed_integrals(ctx, first0 + args.warmup * n_traj, args.steps, stream,
+                                          torch, flush, n_traj)
     if dist:
         dist.barrier()
     clk = clocks.stop()
-    mean_ms = shard.max_over_ranks(sum(ms) / len(ms), dist, "cuda")
+    kmean = ctx.kernel_ms() / args.steps if args.steps * n_traj <= (1 << 22) else call_ms / args.steps
+    mean_ms = shard.max_over_ranks(call_ms / args.steps, dist, "cuda")
     value = world * n_traj / (mean_ms / 1000.0)
-    raw = step_sums.cpu().numpy()
-    sums = [abi.CcsSums.from_buffer_copy(raw[k, :sz].tobytes()) for k in range(args.steps)]
     pot_flops = FLOPS_POT_CHARGED if par.charged else FLOPS_POT_NEUTRAL
-    flops = [FLOPS_LJ * x.pair_lj + FLOPS_ES * x.pair_es + FLOPS_FAR * x.far_terms +
-             pot_flops * x.pair_pot for x in sums]
-    kmean = sum(kern) / len(kern)
-    achieved = sum(flops) / len(flops) / (kmean / 1000.0) / 1e12
+    achieved = (FLOPS_LJ * work.pair_lj + FLOPS_ES * work.pair_es + FLOPS_FAR * work.far_terms +
+                pot_flops * work.pair_pot) / args.steps / (kmean / 1000.0) / 1e12
     fp32_peak, fp64_peak = engine.probe_peaks(local)
     peak = fp32_peak if form == abi.MIXED else fp64_peak
     merged = shard.merge_sums(sums, dist, "cuda")
@@ -711,7 +698,7 @@ def molecule_workload(args, rank, world, local, dist, torch):
                        (f"neutral 128-atom synthetic molecule, force variant {par.force_type}, "
                         f"plain FP64 form, {n_traj} trajectories per step"),
                        "atoms": int(mol.n_atoms), "group_lanes": g,
-                       "l2": "flushed between steps (512 MiB write)"},
+                       "l2": "flushed before the timed call (512 MiB write)"},
             "ccs": {"omega_A2": merged["omega"], "se_A2": merged["se"],
                     "err_pct_mixed_vs_plain": err, "compared_trajectories": n_cmp,
                     "bar_pct": 0.3},
@@ -766,7 +753,7 @@ def main():
                          "neutral 128-atom molecule, 1e4 trajectories, plain FP64 form")
     ap.add_argument("--molecules", type=int, default=256, help="batched/serving: library size")
     ap.add_argument("--rate", type=float, default=0.0,
-                    help="serving: requests per second (0: 80 %% of the measured capacity)")
+                    help="serving: requests per second (0: 75 %% of the measured capacity)")
     ap.add_argument("--duration", type=float, default=120.0, help="serving: seconds of arrivals")
     ap.add_argument("--plain-integrals", type=int, default=3,
                     help="plain FP64 integrals timed beside the mixed line")

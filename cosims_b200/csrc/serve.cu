@@ -21,7 +21,7 @@
 //
 // A job's first chunk is round_traj trajectories (or min_traj); each later
 // chunk is the job's own estimate of what it still needs from its running
-// error (+5 %, at most 16 round_traj).  The chunks are always the next
+// error (+5 %, at most 64 round_traj by default).  The chunks are always the next
 // trajectories of the job's own Philox stream and their sizes follow from the
 // job alone, so its result is the same whether it ran alone or among other
 // jobs, whatever the timing of the rounds.
@@ -42,7 +42,10 @@ namespace {
 
 constexpr int kServeBlock = kBatchMaxBlock;
 constexpr uint32_t kServeImageCap = 96 * 1024;
-constexpr int64_t kMaxChunkRounds = 16;   // default: a chunk is at most 16 round_traj
+// default chunk cap: 64 round_traj.  Against 16 on the configuration-4 mix (3.8
+// requests/s offered, 90 s): p99 latency 20 s instead of 33 s, the 0.2 % requests'
+// median 17 s instead of 27 s, throughput 1.84 M instead of 1.77 M trajectories/s
+constexpr int64_t kMaxChunkRounds = 64;
 constexpr int kRounds = 3;                // rounds in flight at most
 constexpr size_t kArenaAlign = 256;
 constexpr size_t kStageBytes = size_t(8) << 20;   // pinned staging of job images

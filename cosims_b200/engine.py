@@ -395,7 +395,7 @@ class Server:
         check(lib().cosims_serve_release(self._h, job_id))
 
     def set_max_chunk(self, max_chunk_traj: int) -> None:
-        """Largest chunk of one job in one round (0: the default, 16 round_traj)."""
+        """Largest chunk of one job in one round (0: the default, 64 round_traj)."""
         check(lib().cosims_serve_set_max_chunk(self._h, int(max_chunk_traj)))
 
     def info(self) -> tuple:

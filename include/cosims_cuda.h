@@ -189,8 +189,8 @@ cosims_status cosims_ctx_get_launch(const cosims_ctx *ctx, int32_t *group_lanes,
  * integration steps (all attempts) is parked and finished by a wide group
  * once its CTA runs out of other work, so the few very long trajectories no
  * longer set the run time.
- * Mixed form: the wide group is wide_lanes threads (0 = default: 128 up to
- * 1024 atoms, else 256; else a multiple of 32 up to 512); results depend only
+ * Mixed form: the wide group is wide_lanes threads (0 = default: 128; else a
+ * multiple of 32 up to 512); results depend only
  * on the trajectory, group_lanes, step_budget and wide_lanes, not on timing.
  * Default step_budget 2048.
  * Plain form: the wide group is the whole 128-thread CTA (wide_lanes 0 or
@@ -390,7 +390,8 @@ cosims_status cosims_batch_counters(cosims_batch *b, cosims_ccs_sums *work, floa
  * chunk, while rounds run start in the next round without waiting for the
  * others.  A job's first chunk is round_traj trajectories (or min_traj);
  * later chunks are what its running error says it still needs (+5 %, in
- * multiples of round_traj, at most 16 round_traj).  Chunks are the next
+ * multiples of round_traj, at most 64 round_traj by default, see
+ * cosims_serve_set_max_chunk).  Chunks are the next
  * trajectories of the job's own stream and their sizes follow from the job
  * alone, so its result does not depend on the other jobs or on timing.
  * The HBM budget covers the round buffers (3 * max_jobs * round_traj * 76
@@ -427,7 +428,7 @@ cosims_status cosims_serve_poll(cosims_server *s, int64_t job_id, cosims_job_sta
 /* Frees a job's device resources (its slot and footprint return to the pool). */
 cosims_status cosims_serve_release(cosims_server *s, int64_t job_id);
 cosims_status cosims_serve_info(const cosims_server *s, int32_t *active, int64_t *bytes_in_use);
-/* The most trajectories one job integrates in one round (0: the default, 16
+/* The most trajectories one job integrates in one round (0: the default, 64
  * round_traj; at least round_traj).  Larger chunks let jobs that need many
  * trajectories finish in fewer rounds, at the cost of longer rounds for the
  * jobs that share them.  Applies to chunks sized after this call. */
