@@ -162,20 +162,39 @@ bool run_set(cosims_config &cfg, const std::string &mol_path, const std::string 
   std::vector<double> p0(dumps ? 3 * n_traj : 0), v0(dumps ? 3 * n_traj : 0);
   std::vector<int32_t> hit(dumps ? n_traj : 0);
   bool ok = true;
-  for (int k = 0; k < iters; k++) {
+  // Without dumps every integral runs in one cosims_run_integrals call (the
+  // same sums as one call per integral, in fewer launches); each integral's
+  // "Total time" line then shows its share of that call's time.
+  std::vector<cosims_ccs_sums> all(dumps ? 0 : iters);
+  double all_time = 0;
+  if (!dumps) {
+    const auto t0 = std::chrono::steady_clock::now();
+    st = cosims_run_integrals(ctx, (uint64_t)cfg.seed, 0, n_traj, iters, update_every, all.data(),
+                              nullptr, nullptr);
+    all_time = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (st != COSIMS_OK) {
+      out.printf("ERROR: %s\n", cosims_last_error());
+      ok = false;
+    }
+  }
+  for (int k = 0; ok && k < iters; k++) {
     out.printf("\n Computing CCS integral %i / %i on GPU %d (%s form)\n", k + 1, iters, device,
                precision == COSIMS_PRECISION_MIXED ? "mixed" : "plain FP64");
     const auto t0 = std::chrono::steady_clock::now();
     cosims_ccs_sums s;
-    st = cosims_run_sampled(ctx, (uint64_t)cfg.seed, (int64_t)k * n_traj, n_traj, update_every,
-                            &s, dumps ? ins.data() : nullptr, dumps ? outs.data() : nullptr,
-                            nullptr);
+    if (dumps) {
+      st = cosims_run_sampled(ctx, (uint64_t)cfg.seed, (int64_t)k * n_traj, n_traj, update_every,
+                              &s, ins.data(), outs.data(), nullptr);
+    } else {
+      s = all[k];
+    }
     if (st != COSIMS_OK) {
       out.printf("ERROR: %s\n", cosims_last_error());
       ok = false;
       break;
     }
-    total_time += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    total_time += dumps ? std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count()
+                        : all_time / iters;
     if (dumps) {
       // the debugging dumps: successful trajectories, or failed ones with *_fail
       // (the same draws as the integral: its inputs again, with start states and hits)
