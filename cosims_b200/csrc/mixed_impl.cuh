@@ -6,7 +6,7 @@
 // as an FP32 hi/lo pair, so dx = (x_hi - x_atom) + x_lo keeps the separation
 // accurate to FP32 precision of dx itself at close approach.  FP64 is kept for
 // the position/velocity accumulators of the Verlet step, the cluster near/far
-// tests, the energy-conservation check (exact potential, FP64) and the
+// tests, the energy-conservation check (the potential in FP64) and the
 // scattering angle; the CCS sum uses 2 sin^2(chi/2) for 1 - cos(chi).
 //
 // G lanes (1..32) work on one trajectory: they split the atoms, two pairs per
@@ -620,7 +620,22 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
   }
 }
 
-// Exact potential in FP64 (forceAccel.cpp:943-982), lanes split the atoms.
+// 1/sqrt(x) in FP64: the hardware approximation and two Newton steps
+// y <- y (3/2 - x y^2 / 2), each doubling the correct bits (to within a few
+// ulps; no division or square-root sequence).
+__device__ __forceinline__ double rsqrt_f64(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  const double h = 0.5 * x;
+  y = y * fma(-h * y, y, 1.5);
+  y = y * fma(-h * y, y, 1.5);
+  return y;
+}
+
+// The potential in FP64 (forceAccel.cpp:943-982), lanes split the atoms.  The
+// mixed form's energy check needs FP64 accuracy, not the reference's rounding:
+// the powers of 1/r come from one reciprocal square root instead of two IEEE
+// divisions and a square root per atom.
 template <class L>
 __device__ double potential(const View64 &m, const DevParams &p, const double pos[3], L &ln) {
   double v[4] = {0, 0, 0, 0};
@@ -629,11 +644,11 @@ __device__ double potential(const View64 &m, const DevParams &p, const double po
     const double dx = pos[0] - __ldg(A + 0), dy = pos[1] - __ldg(A + 1),
                  dz = pos[2] - __ldg(A + 2);
     const double r2 = dx * dx + dy * dy + dz * dz;
-    const double r6 = r2 * r2 * r2;
-    const double term2 = __ldg(A + 4) / r6;
+    const double ir = rsqrt_f64(r2), ir2 = ir * ir;
+    const double term2 = __ldg(A + 4) * (ir2 * ir2 * ir2);
     v[0] += __ldg(A + 6) * (term2 * term2 - term2);
     if (p.charged) {
-      const double r_3 = __ldg(A + 3) / (r2 * sqrt(r2));
+      const double r_3 = __ldg(A + 3) * (ir * ir2);
       v[1] += dx * r_3; v[2] += dy * r_3; v[3] += dz * r_3;
     }
   }
@@ -1170,11 +1185,11 @@ __device__ __forceinline__ double wide_potential(const View64 &m, const DevParam
     const double dx = pos[0] - __ldg(A + 0), dy = pos[1] - __ldg(A + 1),
                  dz = pos[2] - __ldg(A + 2);
     const double r2 = dx * dx + dy * dy + dz * dz;
-    const double r6 = r2 * r2 * r2;
-    const double term2 = __ldg(A + 4) / r6;
+    const double ir = rsqrt_f64(r2), ir2 = ir * ir;
+    const double term2 = __ldg(A + 4) * (ir2 * ir2 * ir2);
     v[0] += __ldg(A + 6) * (term2 * term2 - term2);
     if (p.charged) {
-      const double r_3 = __ldg(A + 3) / (r2 * sqrt(r2));
+      const double r_3 = __ldg(A + 3) * (ir * ir2);
       v[1] += dx * r_3; v[2] += dy * r_3; v[3] += dz * r_3;
     }
   }
