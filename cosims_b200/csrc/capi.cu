@@ -152,8 +152,26 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   }
   for (int k = 0; k < n; k++) perm[order[k]] = k;
 
+  // F32 slot of each force-order atom: in order, or cluster-blocked (each
+  // cluster from a block start, whole blocks, then one block of padding)
+  const bool blocked = uses && blocked_layout(p->force_type);
+  std::vector<int> slot_of(n), c_slot0(nc + 1, 0);
+  int used = n;
+  if (blocked) {
+    int sidx = 0;
+    for (int c = 0; c < nc; c++) {
+      c_slot0[c] = sidx;
+      for (int k = coff[c]; k < coff[c + 1]; k++) slot_of[k] = sidx + (k - coff[c]);
+      const int sz = coff[c + 1] - coff[c];
+      sidx += (sz + kClusterBlock - 1) / kClusterBlock * kClusterBlock;
+    }
+    c_slot0[nc] = sidx;
+    used = sidx + kClusterBlock;
+  } else {
+    for (int k = 0; k < n; k++) slot_of[k] = k;
+  }
   // F32 arrays padded to a multiple of kSlotQuantum with inert atoms
-  const int ns = (n + kSlotQuantum - 1) / kSlotQuantum * kSlotQuantum;
+  const int ns = (used + kSlotQuantum - 1) / kSlotQuantum * kSlotQuantum;
   std::vector<AtomF64> a64(n);
   std::vector<float4> a4(ns, make_float4(kPadCoord, kPadCoord, kPadCoord, 0.0f));
   // second record: sigma^6, 24 eps/mu, cluster id (integer bits), 0; pad atoms
@@ -162,17 +180,18 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
   uint32_t pad_cid = (uint32_t)nc;
   float pad_cid_f;
   std::memcpy(&pad_cid_f, &pad_cid, 4);
-  for (int k = n; k < ns; k++) b4[k].z = pad_cid_f;
+  for (int k = 0; k < ns; k++) b4[k].z = pad_cid_f;
   for (int k = 0; k < n; k++) {
     const int i = order[k];
     AtomF64 &A = a64[k];
     A.x = m->x[i]; A.y = m->y[i]; A.z = m->z[i]; A.q = m->charge[i];
     A.sig6 = m->sig6[i]; A.eps24m = m->eps24m[i]; A.eps4 = m->eps4[i];
-    a4[k] = make_float4((float)A.x, (float)A.y, (float)A.z, (float)A.q);
+    const int sl = slot_of[k];
+    a4[sl] = make_float4((float)A.x, (float)A.y, (float)A.z, (float)A.q);
     uint32_t ck = (uint32_t)cid[k];
     float ck_f;
     std::memcpy(&ck_f, &ck, 4);
-    b4[k] = make_float4((float)A.sig6, (float)A.eps24m, ck_f, 0.0f);
+    b4[sl] = make_float4((float)A.sig6, (float)A.eps24m, ck_f, 1.0f);
   }
   std::vector<ClusterF64> c64(nc);
   std::vector<ClusterF32> c32(nc);
@@ -201,7 +220,10 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
     for (int k = 0; k < 3; k++) F.dip[k] = (float)C.dip[k];
     for (int k = 0; k < 9; k++) F.quad[k] = (float)C.quad[k];
     F.qsig6 = (float)C.qsig6; F.qeps = (float)C.qeps;
-    F.replaced = C.replaced; F.a0 = C.a0; F.a1 = C.a1;
+    F.replaced = C.replaced;
+    F.a0 = blocked ? c_slot0[c] : C.a0;
+    F.a1 = blocked ? c_slot0[c + 1] : C.a1;
+    F.n_atoms = C.a1 - C.a0;
   }
 
   Builder b64;

@@ -17,13 +17,17 @@
 //     slot before each cluster's atoms for variants 1 and 2.
 //   F32 image (mixed form), variants 1, 2 and 5: in force order, two float4
 //     arrays, (x, y, z, q)
-//     and (sigma^6, 24 eps/mu, cluster id as integer bits, 0), so lanes
-//     reading consecutive atoms hit consecutive banks; ClusterF32 records (FP64
-//     centre and squared radii, so the near/far tests stay FP64; FP32
-//     multipole moments).  The atom arrays are padded to n_slots, a multiple
-//     of kSlotQuantum, with inert atoms (far away, q = sigma^6 = eps = 0,
-//     cluster id n_clusters, whose mode is always 0): every pair term of a pad
-//     atom is exactly zero, so the pair loop needs no bounds test.
+//     and (sigma^6, 24 eps/mu, cluster id as integer bits, 1 for an atom and
+//     0 for padding), so lanes reading consecutive atoms hit consecutive
+//     banks; ClusterF32 records (FP64 centre and squared radii, so the
+//     near/far tests stay FP64; FP32 multipole moments).  The layout is
+//     cluster-blocked: each cluster's atoms start a block of kClusterBlock
+//     slots and fill whole blocks, so the listed-cluster loop reads a
+//     cluster's blocks with no bounds test; the image ends with at least one
+//     block of padding and is padded to n_slots, a multiple of kSlotQuantum.
+//     Padding is inert atoms (far away, q = sigma^6 = eps = 0, cluster id
+//     n_clusters, whose mode is always 0): every pair term of a pad atom is
+//     exactly zero.
 //     Variants 3, 4 and 6 (no far field, no cluster lists) hold the same
 //     values pair-interleaved instead, slots 2j and 2j+1 side by side, as four
 //     arrays over j: (x0, x1, y0, y1), (z0, z1, q0, q1), (sigma^6 0, sigma^6 1,
@@ -40,6 +44,13 @@ constexpr int kMaxAtoms = 16384;
 constexpr int kMaxClusters = 65535;
 constexpr int kMaxGroupLanes = 32;
 constexpr int kSlotQuantum = 2 * kMaxGroupLanes;   // pair loop: two atoms per lane per pass
+constexpr int kClusterBlock = 16;   // blocked F32 layout: a cluster's slots, in whole blocks
+// variants whose F32 image is cluster-blocked: each cluster's atoms start a
+// block of kClusterBlock slots and fill whole blocks (inert padding), and the
+// image ends with at least one block of inert slots
+__host__ __device__ constexpr bool blocked_layout(int force_type) {
+  return force_type == 1 || force_type == 2 || force_type == 5;
+}
 constexpr float kPadCoord = 1.0e6f;                // pad atoms sit this far out (Angstrom)
 constexpr int kMixedMaxBlock = 768;                // threads per CTA of the mixed kernels (80 registers)
 constexpr int kBatchMaxBlock = 768;                // threads per CTA of the batched kernel
@@ -80,8 +91,9 @@ struct ClusterF32 {
   float quad[9];
   float qsig6, qeps;
   int32_t replaced;
-  int32_t a0, a1;
-  int32_t pad[2];
+  int32_t a0, a1;           // slot range (blocked layout: padded to whole blocks)
+  int32_t n_atoms;          // atoms of the cluster (a1 - a0 less the padding)
+  int32_t pad;
 };
 
 static_assert(sizeof(AtomF64) == 56, "AtomF64 layout");

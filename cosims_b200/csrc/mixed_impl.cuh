@@ -395,7 +395,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         const ClusterF32 &C = m.cl[c];
         const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
         in = !(d0 * d0 + d1 * d1 + d2 * d2 > C.dr2);
-        if (TYPE == 5 && in) w.lj += (uint32_t)(C.a1 - C.a0);
+        if (TYPE == 5 && in) w.lj += (uint32_t)C.n_atoms;
         fac[c] = in ? 1.0f : 0.0f;
       }
       const unsigned b = __ballot_sync(0xffffffffu, in);
@@ -453,7 +453,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         } else {
           mode = M_ES | ((TYPE == 2 || in_disp) ? M_LJ : 0);
         }
-        const uint32_t cnt = (uint32_t)(C.a1 - C.a0);
+        const uint32_t cnt = (uint32_t)C.n_atoms;
         if (mode & M_ES) w.es += cnt;
         else if (mode) w.lj += cnt;
       }
@@ -468,20 +468,20 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     }
     ln.sync();
     // pass 2: the listed clusters, two at a time per (half-)group in the two
-    // halves of the packed instructions: lane `sub` takes atom sub (+16 ...)
-    // of both; a cluster without a partner, or the shorter of the two, is
-    // padded in registers with an inert atom (zero charge and prefactor, 1e6 A
-    // away), whose terms are exactly zero
+    // halves of the packed instructions.  The image is cluster-blocked: a
+    // cluster fills whole blocks of kClusterBlock slots, padded with inert
+    // atoms (whose prefactor flag b.w is 0), so lane `sub` walks both
+    // clusters' blocks with no bounds test; a cluster without a partner is
+    // paired with the image's last block, which is all padding
     const int split = G == 32 ? 16 : G;
     const int sub = lane & (split - 1), half = G == 32 ? (lane >> 4) : 0;
     const int step = G == 32 ? 2 : 1;
+    const int inert0 = m.nslots - kClusterBlock;
     Acc2 t = {};
     const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
     const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
-    const float4 inert_a = make_float4(hx + 1.0e6f, hy, hz, 0.0f);
-    const float4 inert_b = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     auto params = [&](const ClusterF32 &C, const float4 &b, uint32_t mode) {
-      if (TYPE == 1 && (mode & M_LJQ)) return f2(C.qsig6, C.qeps);
+      if (TYPE == 1 && (mode & M_LJQ)) return f2(C.qsig6, C.qeps * b.w);
       return f2(b.x, (mode & (M_LJ | M_LJQ)) ? b.y : 0.0f);
     };
     auto run_pairs = [&](int lo, int hi, bool es) {
@@ -494,12 +494,12 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         const int na = CA.a1 - CA.a0, nb = has_b ? CB.a1 - CB.a0 : 0;
         const int nmax = na > nb ? na : nb;
         for (int k = sub; k < nmax; k += split) {
-          const bool ia = k < na, ib = k < nb;
-          const float4 a0 = ia ? m.a4[CA.a0 + k] : inert_a, b0 = ia ? m.b4[CA.a0 + k] : inert_b;
-          const float4 a1 = ib ? m.a4[CB.a0 + k] : inert_a, b1 = ib ? m.b4[CB.a0 + k] : inert_b;
+          const int ka = k < na ? CA.a0 + k : inert0 + (k & (kClusterBlock - 1));
+          const int kb = k < nb ? CB.a0 + k : inert0 + (k & (kClusterBlock - 1));
+          const float4 a0 = m.a4[ka], b0 = m.b4[ka], a1 = m.a4[kb], b1 = m.b4[kb];
           const float2 p0 = params(CA, b0, ea & 0xffu), p1 = params(CB, b1, eb & 0xffu);
-          pair2<TYPE>(a0, a1, f2(ia ? p0.x : 0.0f, ib ? p1.x : 0.0f),
-                      f2(ia ? p0.y : 0.0f, ib ? p1.y : 0.0f), es, hx2, hy2, hz2, lx2, ly2, lz2, t);
+          pair2<TYPE>(a0, a1, f2(p0.x, p1.x), f2(p0.y, p1.y), es, hx2, hy2, hz2, lx2, ly2, lz2,
+                      t);
         }
       }
     };
@@ -540,7 +540,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
       }
       modes[c] = (uint8_t)mode;
       if (Traits<TYPE>::kVaryingPairs) {
-        const uint32_t cnt = (uint32_t)(C.a1 - C.a0);
+        const uint32_t cnt = (uint32_t)C.n_atoms;
         if (mode & M_ES) w.es += cnt;
         else if (mode) w.lj += cnt;
       }
@@ -1093,7 +1093,7 @@ __device__ __forceinline__ void wide_force(const View &m, const DevParams &p, co
       }
       modes[c] = (uint8_t)mode;
       if (Traits<TYPE>::kVaryingPairs) {
-        const uint32_t cnt = (uint32_t)(C.a1 - C.a0);
+        const uint32_t cnt = (uint32_t)C.n_atoms;
         if (mode & M_ES) tl.es += cnt;
         else if (mode) tl.lj += cnt;
       }
