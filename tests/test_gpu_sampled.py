@@ -110,3 +110,27 @@ def test_run_integrals_equals_separate_integrals(name, precision):
     assert work.force_evals == sum(b.force_evals for b in sep)
     assert work.pair_lj + work.pair_es == sum(b.pair_lj + b.pair_es for b in sep)
     assert work.sum == 0 and work.n == 0
+
+
+@pytest.mark.parametrize("precision", [abi.PLAIN_F64, abi.MIXED])
+def test_reserve_allocates_before_the_calls(precision):
+    """cosims_ctx_reserve: after it, calls within the reserved size take no
+    device memory, and their sums equal those of a context that grew its
+    buffers in the calls."""
+    import torch
+    mol, par, _ = load("c0_t5")
+    n, k = 2000, 4
+    with engine.Context(mol, par, precision) as fresh:
+        want, _ = fresh.run_integrals(seed=5, first=0, n_per=n, n_integrals=k)
+    with engine.Context(mol, par, precision) as ctx:
+        ctx.reserve(n * k, k)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        got, _ = ctx.run_integrals(seed=5, first=0, n_per=n, n_integrals=k)
+        ctx.run_sampled(seed=5, first=0, n=n * k)
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free0
+        with pytest.raises(engine.CosimsError):
+            ctx.reserve(-1, 1)
+    for a, b in zip(got, want):
+        assert (a.sum, a.sum2, a.n_hit, a.n_eff) == (b.sum, b.sum2, b.n_hit, b.n_eff)
