@@ -1083,8 +1083,8 @@ __device__ __forceinline__ void wide_force(const View &m, const DevParams &p, co
       } else if (TYPE == 3) {
         mode = M_ES | (in_disp ? M_LJ : 0);
       } else {
+        // far clusters: their far-field terms follow the pair loop
         if (r2 > C.mpr2) {
-          far_terms(m, c, p.multipole_order, (float)d0, (float)d1, (float)d2, s);
           tl.far++;
           mode = TYPE == 2 ? M_LJ : (in_disp ? M_LJQ : 0);
         } else {
@@ -1113,25 +1113,45 @@ __device__ __forceinline__ void wide_force(const View &m, const DevParams &p, co
       }
       fold<TYPE>(t, s);
       k = m.nslots;
-    } else if (!Traits<TYPE>::kFar) {
-      // slots k and k + WG in the two halves of the packed instructions
+    } else if (Traits<TYPE>::kListed) {
+      // cluster-blocked image (variants 1, 2, 5): a 16-lane slice takes two
+      // blocks at a time, one per half of the packed instructions, and skips
+      // pairs of blocks whose clusters add nothing (far field only, or beyond
+      // the cut-off).  A half whose cluster adds no charge field gets charge 0,
+      // so two blocks of different modes share one packed evaluation.
       Acc2 t = {};
       const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
       const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
-#pragma unroll 2
-      for (; k + WG < m.nslots; k += 2 * WG) {
-        const float4 a0 = m.a4[k], b0 = m.b4[k], a1 = m.a4[k + WG], b1 = m.b4[k + WG];
-        const uint32_t m0 = modes[cluster_of(b0)], m1 = modes[cluster_of(b1)];
-        if (Traits<TYPE>::kEsAlways || TYPE == 5 || ((m0 ^ m1) & M_ES) == 0) {
-          const float2 p0 = lj_params<TYPE>(m, b0, m0), p1 = lj_params<TYPE>(m, b1, m1);
-          pair2<TYPE>(a0, a1, f2(p0.x, p1.x), f2(p0.y, p1.y), (m0 & M_ES) != 0, hx2, hy2, hz2,
-                      lx2, ly2, lz2, t);
-        } else {
-          pair<TYPE>(m, a0, b0, m0, hx, hy, hz, lx, ly, lz, s);
-          pair<TYPE>(m, a1, b1, m1, hx, hy, hz, lx, ly, lz, s);
-        }
+      const int sub = lane & (kClusterBlock - 1);
+      const int slices = WG / kClusterBlock;
+      const int nblk = m.nslots / kClusterBlock - 1;      // the last block is padding
+      for (int bA = 2 * (lane / kClusterBlock); bA < nblk; bA += 2 * slices) {
+        const int bB = bA + 1 < nblk ? bA + 1 : nblk;
+        const uint32_t cA = cluster_of(m.b4[bA * kClusterBlock]);
+        const uint32_t cB = cluster_of(m.b4[bB * kClusterBlock]);
+        const uint32_t mA = modes[cA], mB = modes[cB];
+        if ((mA | mB) == 0) continue;
+        const int sA = bA * kClusterBlock + sub, sB = bB * kClusterBlock + sub;
+        const float4 a0 = m.a4[sA], b0 = m.b4[sA], a1 = m.a4[sB], b1 = m.b4[sB];
+        float2 sg, ep;
+        if (TYPE == 1 && (mA & M_LJQ)) { sg.x = m.cl[cA].qsig6; ep.x = m.cl[cA].qeps * b0.w; }
+        else { sg.x = b0.x; ep.x = (mA & (M_LJ | M_LJQ)) ? b0.y : 0.0f; }
+        if (TYPE == 1 && (mB & M_LJQ)) { sg.y = m.cl[cB].qsig6; ep.y = m.cl[cB].qeps * b1.w; }
+        else { sg.y = b1.x; ep.y = (mB & (M_LJ | M_LJQ)) ? b1.y : 0.0f; }
+        const float2 q = f2((mA & M_ES) ? a0.w : 0.0f, (mB & M_ES) ? a1.w : 0.0f);
+        pair2v<TYPE>(f2(a0.x, a1.x), f2(a0.y, a1.y), f2(a0.z, a1.z), q, sg, ep,
+                     ((mA | mB) & M_ES) != 0, hx2, hy2, hz2, lx2, ly2, lz2, t);
       }
       fold<TYPE>(t, s);
+      k = m.nslots;
+      if (Traits<TYPE>::kFar) {
+        for (int c = lane; c < m.nc; c += WG) {
+          if (modes[c] & M_ES) continue;               // near: pair terms above
+          const ClusterF32 &C = m.cl[c];
+          const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
+          far_terms(m, c, p.multipole_order, (float)d0, (float)d1, (float)d2, s);
+        }
+      }
     }
     for (; k < m.nslots; k += WG) {
       const float4 a = m.a4[k], b = m.b4[k];
