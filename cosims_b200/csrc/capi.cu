@@ -194,7 +194,14 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
     b4[sl] = make_float4((float)A.sig6, (float)A.eps24m, ck_f, 1.0f);
   }
   std::vector<ClusterF64> c64(nc);
-  std::vector<ClusterF32> c32(nc);
+  // F32 records: the clusters, then the null cluster (zero moments, centre
+  // 1e4 A away on each axis: its far-field terms are exactly zero)
+  std::vector<ClusterF32> c32(nc + 1);
+  {
+    ClusterF32 &Z = c32[nc];
+    std::memset(&Z, 0, sizeof Z);
+    Z.cx = Z.cy = Z.cz = 1.0e4;
+  }
   for (int c = 0; c < nc; c++) {
     ClusterF64 &C = c64[c];
     std::memset(&C, 0, sizeof C);
@@ -217,7 +224,8 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
     std::memset(&F, 0, sizeof F);
     F.cx = C.cx; F.cy = C.cy; F.cz = C.cz; F.mpr2 = C.mpr2; F.dr2 = C.dr2;
     F.q = (float)C.q;
-    for (int k = 0; k < 3; k++) F.dip[k] = (float)C.dip[k];
+    // a replaced cluster has no dipole term (forceAccel.cpp:258-337)
+    for (int k = 0; k < 3; k++) F.dip[k] = C.replaced ? 0.0f : (float)C.dip[k];
     for (int k = 0; k < 9; k++) F.quad[k] = (float)C.quad[k];
     F.qsig6 = (float)C.qsig6; F.qeps = (float)C.qeps;
     F.replaced = C.replaced;
@@ -278,7 +286,7 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
     i32.off[S_ATOMS] = b32.add(a4.data(), sizeof(float4) * ns);
     i32.off[S_LJ] = b32.add(b4.data(), sizeof(float4) * ns);
   }
-  i32.off[S_CLUSTERS] = b32.add(c32.data(), sizeof(ClusterF32) * nc);
+  i32.off[S_CLUSTERS] = b32.add(c32.data(), sizeof(ClusterF32) * (nc + 1));
   b32.finish();
   i32.bytes = (uint32_t)b32.buf.size();
   i32.n_atoms = n;

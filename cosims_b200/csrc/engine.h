@@ -20,7 +20,10 @@
 //     and (sigma^6, 24 eps/mu, cluster id as integer bits, 1 for an atom and
 //     0 for padding), so lanes reading consecutive atoms hit consecutive
 //     banks; ClusterF32 records (FP64 centre and squared radii, so the
-//     near/far tests stay FP64; FP32 multipole moments).  The layout is
+//     near/far tests stay FP64; FP32 multipole moments, the dipole 0 for a
+//     replaced cluster), then one all-zero record centred 1e4 Angstrom away
+//     on each axis (the null cluster, whose far-field terms are exactly 0:
+//     the partner of an unpaired far cluster in the packed far-field pass).  The layout is
 //     cluster-blocked: each cluster's atoms start a block of kClusterBlock
 //     slots and fill whole blocks, so the listed-cluster loop reads a
 //     cluster's blocks with no bounds test; the image ends with at least one

@@ -290,6 +290,104 @@ __device__ __forceinline__ void fold(const Acc2 &t, Acc &s) {
   }
 }
 
+// Far-field sums of the packed far pass (one cluster per half).
+struct Far2 {
+  float2 Ex, Ey, Ez, Mdx, Mdy, Mdz, Msxy, Msxz, Msyz, Maxy, Maxz, Mayz;
+};
+
+__device__ __forceinline__ float2 neg2(const float2 &a) { return f2(-a.x, -a.y); }
+// far_terms for two clusters at once, one per half of the packed
+// instructions (the distance is the FP64 difference rounded to FP32, as in
+// far_terms).  Replaced clusters carry a zero dipole in the F32 image; the
+// null cluster (index n_clusters: zero moments, centre 1e4 Angstrom away on
+// each axis) adds exactly 0, so it fills a half that has no far cluster.
+__device__ __forceinline__ void far2(const View &m, int ia, int ib, int order,
+                                     const double pos[3], Far2 &s) {
+  const ClusterF32 &A = m.cl[ia];
+  const ClusterF32 &B = m.cl[ib];
+  const float2 dx = f2((float)(pos[0] - A.cx), (float)(pos[0] - B.cx));
+  const float2 dy = f2((float)(pos[1] - A.cy), (float)(pos[1] - B.cy));
+  const float2 dz = f2((float)(pos[2] - A.cz), (float)(pos[2] - B.cz));
+  const float2 xx = __fmul2_rn(dx, dx), yy = __fmul2_rn(dy, dy), zz = __fmul2_rn(dz, dz);
+  const float2 r2 = __fadd2_rn(__fadd2_rn(xx, yy), zz);
+  const float2 r_1 = f2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+  const float2 r_2 = __fmul2_rn(r_1, r_1);
+  const float2 r_3 = __fmul2_rn(r_2, r_1);
+  const float2 r_5 = __fmul2_rn(r_3, r_2);
+  const float2 xy = __fmul2_rn(dx, dy), xz = __fmul2_rn(dx, dz), yz = __fmul2_rn(dy, dz);
+  const float2 cR5 = __fmul2_rn(f2(A.q, B.q), r_5);
+  const float2 cR3 = __fmul2_rn(cR5, r2);
+  const float2 m3 = f2(-3.0f, -3.0f);
+  s.Ex = __ffma2_rn(cR3, dx, s.Ex);
+  s.Ey = __ffma2_rn(cR3, dy, s.Ey);
+  s.Ez = __ffma2_rn(cR3, dz, s.Ez);
+  s.Mdx = __ffma2_rn(__ffma2_rn(m3, xx, r2), cR5, s.Mdx);
+  s.Mdy = __ffma2_rn(__ffma2_rn(m3, yy, r2), cR5, s.Mdy);
+  s.Mdz = __ffma2_rn(__ffma2_rn(m3, zz, r2), cR5, s.Mdz);
+  s.Msxy = __ffma2_rn(__fmul2_rn(m3, xy), cR5, s.Msxy);
+  s.Msxz = __ffma2_rn(__fmul2_rn(m3, xz), cR5, s.Msxz);
+  s.Msyz = __ffma2_rn(__fmul2_rn(m3, yz), cR5, s.Msyz);
+  if (order >= 1) {
+    const float2 D0 = f2(A.dip[0], B.dip[0]), D1 = f2(A.dip[1], B.dip[1]),
+                 D2 = f2(A.dip[2], B.dip[2]);
+    const float2 r_7 = __fmul2_rn(r_5, r_2);
+    const float2 c1 = __fmul2_rn(f2(3.0f, 3.0f),
+                                 __ffma2_rn(D2, dz, __ffma2_rn(D1, dy, __fmul2_rn(D0, dx))));
+    const float2 nr2 = neg2(r2);
+    s.Ex = __ffma2_rn(__ffma2_rn(c1, dx, __fmul2_rn(nr2, D0)), r_5, s.Ex);
+    s.Ey = __ffma2_rn(__ffma2_rn(c1, dy, __fmul2_rn(nr2, D1)), r_5, s.Ey);
+    s.Ez = __ffma2_rn(__ffma2_rn(c1, dz, __fmul2_rn(nr2, D2)), r_5, s.Ez);
+    const float2 r7c1 = __fmul2_rn(r_7, c1);
+    const float2 m5 = f2(-5.0f, -5.0f);
+    s.Mdx = __ffma2_rn(__ffma2_rn(m5, xx, r2), r7c1, s.Mdx);
+    s.Mdy = __ffma2_rn(__ffma2_rn(m5, yy, r2), r7c1, s.Mdy);
+    s.Mdz = __ffma2_rn(__ffma2_rn(m5, zz, r2), r7c1, s.Mdz);
+    s.Msxy = __ffma2_rn(__fmul2_rn(m5, xy), r7c1, s.Msxy);
+    s.Msxz = __ffma2_rn(__fmul2_rn(m5, xz), r7c1, s.Msxz);
+    s.Msyz = __ffma2_rn(__fmul2_rn(m5, yz), r7c1, s.Msyz);
+    const float2 r5_3 = __fmul2_rn(f2(3.0f, 3.0f), r_5);
+    s.Maxy = __ffma2_rn(__ffma2_rn(D1, dx, __fmul2_rn(neg2(D0), dy)), r5_3, s.Maxy);
+    s.Maxz = __ffma2_rn(__ffma2_rn(D2, dx, __fmul2_rn(neg2(D0), dz)), r5_3, s.Maxz);
+    s.Mayz = __ffma2_rn(__ffma2_rn(D2, dy, __fmul2_rn(neg2(D1), dz)), r5_3, s.Mayz);
+  }
+  if (order >= 2) {
+    const float *QA = A.quad, *QB = B.quad;
+    const float2 r_7 = __fmul2_rn(r_5, r_2);
+    const float2 t0 = __fmul2_rn(__ffma2_rn(f2(QA[6], QB[6]), dz,
+                                  __ffma2_rn(f2(QA[3], QB[3]), dy, __fmul2_rn(f2(QA[0], QB[0]), dx))), r_7);
+    const float2 t1 = __fmul2_rn(__ffma2_rn(f2(QA[7], QB[7]), dz,
+                                  __ffma2_rn(f2(QA[4], QB[4]), dy, __fmul2_rn(f2(QA[1], QB[1]), dx))), r_7);
+    const float2 t2 = __fmul2_rn(__ffma2_rn(f2(QA[8], QB[8]), dz,
+                                  __ffma2_rn(f2(QA[5], QB[5]), dy, __fmul2_rn(f2(QA[2], QB[2]), dx))), r_7);
+    const float2 c2 = __fmul2_rn(__fmul2_rn(f2(2.5f, 2.5f),
+                                            __ffma2_rn(t2, dz, __ffma2_rn(t1, dy, __fmul2_rn(t0, dx)))),
+                                 r_2);
+    s.Ex = __ffma2_rn(__ffma2_rn(c2, dx, neg2(t0)), r2, s.Ex);
+    s.Ey = __ffma2_rn(__ffma2_rn(c2, dy, neg2(t1)), r2, s.Ey);
+    s.Ez = __ffma2_rn(__ffma2_rn(c2, dz, neg2(t2)), r2, s.Ez);
+    const float2 m7 = f2(-7.0f, -7.0f);
+    s.Mdx = __ffma2_rn(__ffma2_rn(m7, xx, r2), c2, __ffma2_rn(neg2(f2(QA[0], QB[0])), r_5, s.Mdx));
+    s.Mdy = __ffma2_rn(__ffma2_rn(m7, yy, r2), c2, __ffma2_rn(neg2(f2(QA[4], QB[4])), r_5, s.Mdy));
+    s.Mdz = __ffma2_rn(__ffma2_rn(m7, zz, r2), c2, __ffma2_rn(neg2(f2(QA[8], QB[8])), r_5, s.Mdz));
+    s.Msxy = __ffma2_rn(__fmul2_rn(m7, xy), c2, __ffma2_rn(neg2(f2(QA[1], QB[1])), r_5, s.Msxy));
+    s.Msxz = __ffma2_rn(__fmul2_rn(m7, xz), c2, __ffma2_rn(neg2(f2(QA[2], QB[2])), r_5, s.Msxz));
+    s.Msyz = __ffma2_rn(__fmul2_rn(m7, yz), c2, __ffma2_rn(neg2(f2(QA[5], QB[5])), r_5, s.Msyz));
+    const float2 p5 = f2(5.0f, 5.0f);
+    s.Maxy = __ffma2_rn(p5, __ffma2_rn(t1, dx, __fmul2_rn(neg2(t0), dy)), s.Maxy);
+    s.Maxz = __ffma2_rn(p5, __ffma2_rn(t2, dx, __fmul2_rn(neg2(t0), dz)), s.Maxz);
+    s.Mayz = __ffma2_rn(p5, __ffma2_rn(t2, dy, __fmul2_rn(neg2(t1), dz)), s.Mayz);
+  }
+}
+
+// The 12 far-field sums of a lane (both halves added), in the order of the
+// group reduction: E (3), then the nine far-field gradient terms.
+__device__ __forceinline__ void far_values(const Far2 &t, float (&v)[12]) {
+  v[0] = t.Ex.x + t.Ex.y; v[1] = t.Ey.x + t.Ey.y; v[2] = t.Ez.x + t.Ez.y;
+  v[3] = t.Mdx.x + t.Mdx.y; v[4] = t.Mdy.x + t.Mdy.y; v[5] = t.Mdz.x + t.Mdz.y;
+  v[6] = t.Msxy.x + t.Msxy.y; v[7] = t.Msxz.x + t.Msxz.y; v[8] = t.Msyz.x + t.Msyz.y;
+  v[9] = t.Maxy.x + t.Maxy.y; v[10] = t.Maxz.x + t.Maxz.y; v[11] = t.Mayz.x + t.Mayz.y;
+}
+
 struct WorkM { uint32_t lj, es, far; };
 
 // Reduce-scatter of K values over a group of G lanes (G a power of two <= 32,
@@ -370,11 +468,18 @@ struct NarrowLanes {
 
 // Acceleration at pos (FP64 in, FP64 out) for one group.  Pair counts are
 // taken per cluster in pass 1 (or per evaluation), not per pair.
-template <int TYPE, class L>
+// PACKED_FAR: the far field of variants 1 and 2 in packed instructions, for
+// kernels with the registers for it (the single-molecule kernel at 512
+// threads); the batched kernel, at 80 registers, keeps the scalar pass.
+template <int TYPE, bool PACKED_FAR, class L>
 __device__ __forceinline__ void force(const View &m, const DevParams &p, const double pos[3],
                                       double acc[3], L &ln, uint8_t *modes, WorkM &w) {
   const int G = ln.G, lane = ln.lane;
   Acc s = {};
+  // far-field sums already reduced over the group (listed variants 1 and 2
+  // with G >= 16): this lane's share of the 12, see the far pass
+  float far_share = 0.0f;
+  bool far_reduced = false;
   const float hx = (float)pos[0], hy = (float)pos[1], hz = (float)pos[2];
   const float lx = (float)(pos[0] - (double)hx), ly = (float)(pos[1] - (double)hy),
               lz = (float)(pos[2] - (double)hz);
@@ -437,7 +542,8 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     const unsigned gbits = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
     const unsigned below = (1u << lane) - 1u;
     int n_es = 0, n_lj = 0;
-    for (int c0 = 0; c0 < m.nc; c0 += G) {
+    unsigned long long far_bits = 0;       // bit i: cluster lane + i G is far
+    for (int c0 = 0, it = 0; c0 < m.nc; c0 += G, it++) {
       const int c = c0 + lane;
       uint32_t mode = 0;
       if (c < m.nc) {
@@ -449,6 +555,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
           mode = in_disp ? M_LJ : 0;
         } else if (r2 > C.mpr2) {
           w.far++;
+          if (it < 64) far_bits |= 1ull << it;
           mode = TYPE == 2 ? M_LJ : (in_disp ? M_LJQ : 0);
         } else {
           mode = M_ES | ((TYPE == 2 || in_disp) ? M_LJ : 0);
@@ -467,6 +574,32 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
       n_lj += __popc(m_lj);
     }
     ln.sync();
+    // far field first (variants 1 and 2, G >= 16): a lane takes its clusters
+    // lane + i G two at a time, one per half of the packed instructions, with
+    // pass 1's decisions (recomputed past 64 rounds); a half without a far
+    // cluster takes the null cluster, which adds 0.  The 12 sums are reduced
+    // over the group at once (reduce-scatter: one value per lane), so the
+    // pair loop below runs with one extra register instead of 24.
+    if (Traits<TYPE>::kFar && PACKED_FAR && G >= 16) {
+      Far2 f = {};
+      auto is_far = [&](int c, int it) {
+        if (c >= m.nc) return false;
+        if (it < 64) return ((far_bits >> it) & 1ull) != 0;
+        const ClusterF32 &C = m.cl[c];
+        const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
+        return d0 * d0 + d1 * d1 + d2 * d2 > C.mpr2;
+      };
+      for (int c = lane, it = 0; c < m.nc; c += 2 * G, it += 2) {
+        const bool fa = is_far(c, it), fb = is_far(c + G, it + 1);
+        if (!(fa || fb)) continue;
+        far2(m, fa ? c : m.nc, fb ? c + G : m.nc, p.multipole_order, pos, f);
+      }
+      float fv[12];
+      far_values(f, fv);
+      int idx;
+      far_share = reduce_scatter<12>(fv, G, lane, idx);
+      far_reduced = true;
+    }
     // pass 2: the listed clusters, two at a time per (half-)group in the two
     // halves of the packed instructions.  The image is cluster-blocked: a
     // cluster fills whole blocks of kClusterBlock slots, padded with inert
@@ -506,9 +639,9 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     if (Traits<TYPE>::kCharge) run_pairs(0, n_es, true);
     run_pairs(m.nc - n_lj, m.nc, false);
     fold<TYPE>(t, s);
-    // pass 3: the far field of the far clusters (multipole variants), after the
-    // pair sums are folded, so the pair loop keeps its registers for them
-    if (Traits<TYPE>::kFar) {
+    // pass 3 (G < 16): the far field of the far clusters, after the pair
+    // sums are folded, so the pair loop keeps its registers for them
+    if (Traits<TYPE>::kFar && !far_reduced) {
       for (int c = lane; c < m.nc; c += G) {
         const ClusterF32 &C = m.cl[c];
         const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
@@ -589,6 +722,31 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     fold<TYPE>(t, s);
   }
   // group reduction (identical result in every lane of the group)
+  if (Traits<TYPE>::kFar && far_reduced) {
+    // the 13 pair sums, then the far sums from the lanes that hold them
+    float v[13];
+    v[0] = s.Fx; v[1] = s.Fy; v[2] = s.Fz;
+    v[3] = s.Ex; v[4] = s.Ey; v[5] = s.Ez;
+    v[6] = s.Pxx; v[7] = s.Pxy; v[8] = s.Pxz; v[9] = s.Pyy; v[10] = s.Pyz; v[11] = s.Pzz;
+    v[12] = s.Q3;
+    ln.sum(v);
+    float fv[12];
+    const int gbase = (threadIdx.x & 31) & ~(G - 1);
+    const int stride = G / 16;
+#pragma unroll
+    for (int k = 0; k < 12; k++) fv[k] = __shfl_sync(0xffffffffu, far_share, gbase + k * stride);
+    acc[0] = v[0]; acc[1] = v[1]; acc[2] = v[2];
+    const double Mxx = (double)v[12] - 3.0 * v[6] + fv[3], Myy = (double)v[12] - 3.0 * v[9] + fv[4],
+                 Mzz = (double)v[12] - 3.0 * v[11] + fv[5];
+    const double Sxy = -3.0 * v[7] + fv[6], Sxz = -3.0 * v[8] + fv[7], Syz = -3.0 * v[10] + fv[8];
+    const double Axy = fv[9], Axz = fv[10], Ayz = fv[11];
+    const double Ex = (double)v[3] + fv[0], Ey = (double)v[4] + fv[1], Ez = (double)v[5] + fv[2];
+    const double ds = p.dipole_scalar;
+    acc[0] += ds * (Mxx * Ex + (Sxy + Axy) * Ey + (Sxz + Axz) * Ez);
+    acc[1] += ds * ((Sxy - Axy) * Ex + Myy * Ey + (Syz + Ayz) * Ez);
+    acc[2] += ds * ((Sxz - Axz) * Ex + (Syz - Ayz) * Ey + Mzz * Ez);
+    return;
+  }
   constexpr int K = Traits<TYPE>::kFar ? 22 : (Traits<TYPE>::kCharge ? 13 : 3);
   float v[K];
   v[0] = s.Fx; v[1] = s.Fy; v[2] = s.Fz;
@@ -757,6 +915,10 @@ struct ArgsSource {
   const TrajArgs &a;
 };
 
+// Whether a source's kernel takes the packed far-field pass (see force).
+template <class Src> struct PackedFar { static constexpr bool value = false; };
+template <> struct PackedFar<ArgsSource> { static constexpr bool value = true; };
+
 __device__ __forceinline__ cosims_traj_out *out_of(const MainSource &s) { return s.out; }
 __device__ __forceinline__ cosims_traj_out *out_of(const ArgsSource &s) { return s.a.out; }
 __device__ __forceinline__ long long budget_of(const MainSource &s) { return s.ho.budget; }
@@ -871,7 +1033,7 @@ __device__ __forceinline__ void group_loop(const View &m, const View64 &m64, con
 
     double an[3];
     WorkM wi = {0, 0, 0};
-    force<TYPE>(m, p, ep, an, ln, modes, wi);
+    force<TYPE, PackedFar<Src>::value>(m, p, ep, an, ln, modes, wi);
     if (Traits<TYPE>::kVaryingPairs) {
       tl.lj += wi.lj; tl.es += wi.es; tl.far += wi.far;
     }
@@ -1420,11 +1582,13 @@ __device__ __noinline__ void wide_phase(unsigned char *smem, uint32_t img_bytes,
 }
 
 // Threads per CTA at most: 768 gives 80 registers a thread, enough for the
-// wide groups' register-resident state and the far-field sums of variants 1
-// and 2 (the narrow phase runs as fast at 24 warps per SM as at 32).
+// wide groups' register-resident state (the narrow phase runs as fast at 24
+// warps per SM as at 32).  The far-field variants 1 and 2 take 512 threads
+// and 128 registers: their packed far-field pass holds 12 packed sums and
+// the multipole temporaries, which spill at 80.
 template <int TYPE>
 struct KernelShape {
-  static constexpr int kMaxThreads = kMixedMaxBlock;
+  static constexpr int kMaxThreads = (TYPE == 1 || TYPE == 2) ? 512 : kMixedMaxBlock;
 };
 
 // SMEM: the F32 image is staged in shared memory (else read from global
