@@ -297,17 +297,14 @@ struct Far2 {
 
 __device__ __forceinline__ float2 neg2(const float2 &a) { return f2(-a.x, -a.y); }
 // far_terms for two clusters at once, one per half of the packed
-// instructions (the distance is the FP64 difference rounded to FP32, as in
-// far_terms).  Replaced clusters carry a zero dipole in the F32 image; the
-// null cluster (index n_clusters: zero moments, centre 1e4 Angstrom away on
-// each axis) adds exactly 0, so it fills a half that has no far cluster.
-__device__ __forceinline__ void far2(const View &m, int ia, int ib, int order,
-                                     const double pos[3], Far2 &s) {
+// instructions, from their distances (the FP64 differences rounded to FP32,
+// as in far_terms).  Replaced clusters carry a zero dipole in the F32 image;
+// the null cluster (index n_clusters, zero moments) adds exactly 0 at any
+// finite distance, so it fills a half that has no far cluster.
+__device__ __forceinline__ void far2(const View &m, int ia, int ib, int order, const float2 &dx,
+                                     const float2 &dy, const float2 &dz, Far2 &s) {
   const ClusterF32 &A = m.cl[ia];
   const ClusterF32 &B = m.cl[ib];
-  const float2 dx = f2((float)(pos[0] - A.cx), (float)(pos[0] - B.cx));
-  const float2 dy = f2((float)(pos[1] - A.cy), (float)(pos[1] - B.cy));
-  const float2 dz = f2((float)(pos[2] - A.cz), (float)(pos[2] - B.cz));
   const float2 xx = __fmul2_rn(dx, dx), yy = __fmul2_rn(dy, dy), zz = __fmul2_rn(dz, dz);
   const float2 r2 = __fadd2_rn(__fadd2_rn(xx, yy), zz);
   const float2 r_1 = f2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
@@ -542,10 +539,12 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     const unsigned gbits = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
     const unsigned below = (1u << lane) - 1u;
     int n_es = 0, n_lj = 0;
-    unsigned long long far_bits = 0;       // bit i: cluster lane + i G is far
-    for (int c0 = 0, it = 0; c0 < m.nc; c0 += G, it++) {
+    // one round: the clusters c0 + lane; returns whether the lane's cluster
+    // is far, with its distance rounded to FP32
+    auto classify = [&](int c0, float &fx, float &fy, float &fz) {
       const int c = c0 + lane;
       uint32_t mode = 0;
+      bool far = false;
       if (c < m.nc) {
         const ClusterF32 &C = m.cl[c];
         const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
@@ -555,7 +554,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
           mode = in_disp ? M_LJ : 0;
         } else if (r2 > C.mpr2) {
           w.far++;
-          if (it < 64) far_bits |= 1ull << it;
+          far = true;
           mode = TYPE == 2 ? M_LJ : (in_disp ? M_LJQ : 0);
         } else {
           mode = M_ES | ((TYPE == 2 || in_disp) ? M_LJ : 0);
@@ -563,6 +562,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         const uint32_t cnt = (uint32_t)C.n_atoms;
         if (mode & M_ES) w.es += cnt;
         else if (mode) w.lj += cnt;
+        fx = (float)d0; fy = (float)d1; fz = (float)d2;
       }
       const bool es = (mode & M_ES) != 0, ljo = mode != 0 && !es;
       const unsigned m_es = (__ballot_sync(0xffffffffu, es) >> gbase) & gbits;
@@ -572,34 +572,38 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
       if (ljo) list[m.nc - 1 - n_lj - __popc(m_lj & below)] = e;
       n_es += __popc(m_es);
       n_lj += __popc(m_lj);
-    }
-    ln.sync();
-    // far field first (variants 1 and 2, G >= 16): a lane takes its clusters
-    // lane + i G two at a time, one per half of the packed instructions, with
-    // pass 1's decisions (recomputed past 64 rounds); a half without a far
-    // cluster takes the null cluster, which adds 0.  The 12 sums are reduced
-    // over the group at once (reduce-scatter: one value per lane), so the
-    // pair loop below runs with one extra register instead of 24.
+      return far;
+    };
     if (Traits<TYPE>::kFar && PACKED_FAR && G >= 16) {
+      // far field in the same pass (variants 1 and 2, G >= 16): two rounds
+      // at a time, the lane's far cluster of each in one half of the packed
+      // instructions (the null cluster fills a half without one).  The 12
+      // sums are reduced over the group at once (reduce-scatter: one value
+      // per lane), so the pair loop below runs with one extra register
+      // instead of 24.
       Far2 f = {};
-      auto is_far = [&](int c, int it) {
-        if (c >= m.nc) return false;
-        if (it < 64) return ((far_bits >> it) & 1ull) != 0;
-        const ClusterF32 &C = m.cl[c];
-        const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
-        return d0 * d0 + d1 * d1 + d2 * d2 > C.mpr2;
-      };
-      for (int c = lane, it = 0; c < m.nc; c += 2 * G, it += 2) {
-        const bool fa = is_far(c, it), fb = is_far(c + G, it + 1);
-        if (!(fa || fb)) continue;
-        far2(m, fa ? c : m.nc, fb ? c + G : m.nc, p.multipole_order, pos, f);
+      for (int c0 = 0; c0 < m.nc; c0 += 2 * G) {
+        float ax = 1.0e4f, ay = 1.0e4f, az = 1.0e4f, bx = 1.0e4f, by = 1.0e4f, bz = 1.0e4f;
+        const bool fa = classify(c0, ax, ay, az);
+        const bool fb = c0 + G < m.nc ? classify(c0 + G, bx, by, bz) : false;
+        if (!fa) ax = ay = az = 1.0e4f;
+        if (!fb) bx = by = bz = 1.0e4f;
+        if (fa || fb)
+          far2(m, fa ? c0 + lane : m.nc, fb ? c0 + G + lane : m.nc, p.multipole_order,
+               f2(ax, bx), f2(ay, by), f2(az, bz), f);
       }
       float fv[12];
       far_values(f, fv);
       int idx;
       far_share = reduce_scatter<12>(fv, G, lane, idx);
       far_reduced = true;
+    } else {
+      for (int c0 = 0; c0 < m.nc; c0 += G) {
+        float x, y, z;
+        classify(c0, x, y, z);
+      }
     }
+    ln.sync();
     // pass 2: the listed clusters, two at a time per (half-)group in the two
     // halves of the packed instructions.  The image is cluster-blocked: a
     // cluster fills whole blocks of kClusterBlock slots, padded with inert
