@@ -748,7 +748,9 @@ cosims_status cosims_ctx_set_launch(cosims_ctx *c, int32_t group_lanes, int32_t 
     c->group_lanes = group_lanes;
   }
   if (block_threads) {
-    const int maxb = c->precision == COSIMS_PRECISION_PLAIN_F64 ? 128 : kMixedMaxBlock;
+    const int maxb = c->precision == COSIMS_PRECISION_PLAIN_F64 ? 128
+                     : (c->par.force_type == 1 || c->par.force_type == 2) ? kMixedFarBlock
+                                                                         : kMixedMaxBlock;
     if (block_threads < 32 || block_threads > maxb || (block_threads & 31))
       return fail(COSIMS_ERR_INVALID, "block_threads must be a multiple of 32 in 32..%d", maxb);
     c->block_threads = block_threads;

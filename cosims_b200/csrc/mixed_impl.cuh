@@ -466,8 +466,8 @@ struct NarrowLanes {
 // Acceleration at pos (FP64 in, FP64 out) for one group.  Pair counts are
 // taken per cluster in pass 1 (or per evaluation), not per pair.
 // PACKED_FAR: the far field of variants 1 and 2 in packed instructions, for
-// kernels with the registers for it (the single-molecule kernel at 512
-// threads); the batched kernel, at 80 registers, keeps the scalar pass.
+// kernels with the registers for it (the single-molecule kernel of those
+// variants and the batched kernel run 512-thread CTAs at 128 registers).
 template <int TYPE, bool PACKED_FAR, class L>
 __device__ __forceinline__ void force(const View &m, const DevParams &p, const double pos[3],
                                       double acc[3], L &ln, uint8_t *modes, WorkM &w) {
@@ -1592,7 +1592,7 @@ __device__ __noinline__ void wide_phase(unsigned char *smem, uint32_t img_bytes,
 // the multipole temporaries, which spill at 80.
 template <int TYPE>
 struct KernelShape {
-  static constexpr int kMaxThreads = (TYPE == 1 || TYPE == 2) ? 512 : kMixedMaxBlock;
+  static constexpr int kMaxThreads = (TYPE == 1 || TYPE == 2) ? kMixedFarBlock : kMixedMaxBlock;
 };
 
 // SMEM: the F32 image is staged in shared memory (else read from global
