@@ -1102,7 +1102,10 @@ __device__ __forceinline__ void group_loop(const View &m, const View64 &m64, con
     } else if (outside && step > 10) {
       const double endE = U + 0.5 * p.mu * dot3(vel, vel);
       dE = 100 * fabs(E0 - endE) / E0;
-      if (dE > 0.5) {
+      // a non-finite energy fails the check: a pair term that overflows FP32
+      // at a near collision leaves inf or NaN where FP64 holds a huge, finite
+      // energy error, which fails it (diffEqSolver.cpp:188-194)
+      if (!(dE <= 0.5)) {
         tries++;
         max_tries++;
         etries++;
@@ -1116,8 +1119,9 @@ __device__ __forceinline__ void group_loop(const View &m, const View64 &m64, con
       }
     }
     if (!finished) {
-      // the step cap, or a state gone non-finite (the reference would loop)
-      if (total >= cap || !isfinite(rdot)) {
+      // the step cap, or a state gone non-finite (the reference would loop);
+      // a step whose energy check just failed retries instead
+      if (total >= cap || (!isfinite(rdot) && step_out != 0)) {
         chi = COSIMS_PI_2; dE = 0.0;
         status = COSIMS_TRAJ_HIT | COSIMS_TRAJ_STEPCAP;
         finished = true;
@@ -1493,7 +1497,7 @@ __device__ __forceinline__ void wide_loop(const View &m, const View64 &m64, cons
         const double E0 = __ldcg(&R->E0);
         const double endE = U + 0.5 * p.mu * dot3(vel, vel);
         dE = 100 * fabs(E0 - endE) / E0;
-        if (dE > 0.5) {
+        if (!(dE <= 0.5)) {                    // non-finite fails, as in the narrow loop
           tries++;
           max_tries++;
           etries++;
@@ -1509,7 +1513,7 @@ __device__ __forceinline__ void wide_loop(const View &m, const View64 &m64, cons
         }
       }
       if (!finished) {
-        if (total >= cap || !isfinite(rdot)) {
+        if (total >= cap || (!isfinite(rdot) && step != 0)) {
           status |= COSIMS_TRAJ_STEPCAP;
           finished = true;
         } else if (!(tries < max_tries && max_tries < 10)) {
