@@ -42,9 +42,13 @@ def test_mixed_vs_reference_list(name):
     assert abs(c_mix - c_ref) / c_ref < max(CCS_TOL, 2.0 / len(p0))
 
 
-@pytest.mark.parametrize("group_lanes", [1, 4, 8, 32])
-def test_mixed_group_shapes_agree(group_lanes):
-    mol, par, d = load("q128_t1")
+@pytest.mark.parametrize("group_lanes", [1, 4, 8, 16, 32])
+@pytest.mark.parametrize("name", ["q128_t1", "q128_t1_o0", "q128_t2"])
+def test_mixed_group_shapes_agree(name, group_lanes):
+    """Every lane count against the reference's chi; for the far-field
+    variants 1 and 2, 16 and 32 lanes take the packed far-field pass (multipole
+    orders 1, 0 and 2 here) and fewer lanes the scalar one."""
+    mol, par, d = load(name)
     p0, v0 = hits(d)
     with engine.Context(mol, par, abi.MIXED) as ctx:
         ctx.set_launch(group_lanes=group_lanes)
@@ -64,3 +68,19 @@ def test_mixed_ccs_within_tolerance_of_plain(name, n):
     assert abs(sm.sum - sp.sum) / sp.sum < CCS_TOL
     hit = (op["status"] & abi.TRAJ_HIT) > 0
     assert np.median(np.abs(op["chi"][hit] - om["chi"][hit])) < 1e-4
+
+
+@pytest.mark.parametrize("name", ["q128_t1", "q128_t2"])
+def test_packed_far_field_ccs_within_tolerance_of_plain(name):
+    """The packed far-field pass (16 and 32 lanes) against the plain form on
+    the same sampled inputs, as the scalar pass is above."""
+    mol, par, _ = load(name)
+    n = 20000
+    with engine.Context(mol, par, abi.PLAIN_F64) as cp:
+        sp, _, _ = cp.run_sampled(seed=99, first=0, n=n)
+    for lanes in (16, 32):
+        with engine.Context(mol, par, abi.MIXED) as cm:
+            cm.set_launch(group_lanes=lanes)
+            sm, _, _ = cm.run_sampled(seed=99, first=0, n=n)
+        assert sm.n_hit == sp.n_hit
+        assert abs(sm.sum - sp.sum) / sp.sum < CCS_TOL
