@@ -2,10 +2,10 @@
 //
 // impactParam::setBoundry (impactParam.cpp:663-721) marches 20 rays per z
 // level inward in 0.1 Angstrom steps until the potential reaches -1 % of the
-// slowest kinetic energy.  Each ray is independent: one thread per ray here,
-// with the potential summed in file order in IEEE double (this file is
-// compiled with --fmad=false), so every boundary point equals the host's bit
-// for bit.  Ray starts and directions are the host's (libm cos/sin).  A ray
+// slowest kinetic energy.  Each ray is independent: one warp per ray here,
+// each lane one step of the ray, with the potential summed in file order in
+// IEEE double (this file is compiled with --fmad=false), so every boundary
+// point equals the host's bit for bit.  Ray starts and directions are the host's (libm cos/sin).  A ray
 // that runs past kMaxSteps stops and flags an error instead of looping.
 #include <cuda_runtime.h>
 #include <cstdio>
@@ -46,40 +46,69 @@ __device__ __forceinline__ double mag3(double x, double y, double z) {
   return sqrt((x * x) + (y * y) + (z * z));
 }
 
+// One warp per ray.  The march is sequential only in its stopping point, so
+// the warp evaluates 32 consecutive steps at once, one per lane, and stops at
+// the first lane whose step meets a stop condition.  Lane l's position is the
+// chunk's base position plus l additions of the step vector: the same
+// sequence of roundings as the serial march (px = px + vx each step), so the
+// positions, potentials and the boundary point are the host's bit for bit.
+// The steps after the stopping one are evaluated and discarded.
 __global__ void boundary_rays(const RayAtoms m, int charged, double ds, double minKin, double zMax,
                               double zInc, int levels, int rotations, const double *sx,
                               const double *sy, const double *vx, const double *vy, double *out,
                               int *err) {
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= levels * rotations) return;
+  const int r = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  if (r >= levels * rotations) return;           // whole warps: r is warp-uniform
   const int i = r / rotations, n = r % rotations;
   const double zPos = -zMax + i * zInc;
   const double startX = sx[n], startY = sy[n];
-  double px = startX, py = startY, pz = zPos;
   double vxs = vx[n], vys = vy[n], vzs = 0.0;
   double sl = 1;
-  double e = ray_potential(m, charged, ds, px, py, pz);
-  if (e + minKin < 0) sl = -1;
+  const double e0 = ray_potential(m, charged, ds, startX, startY, zPos);
+  if (e0 + minKin < 0) sl = -1;
   vxs = vxs * sl; vys = vys * sl; vzs = vzs * sl;
-  double qx = 0, qy = 0, qz = 0;                      // prevPos
+  double bx = startX, by = startY, bz = zPos;       // position of the chunk's first step
+  double qx = 0, qy = 0, qz = 0;                    // position of the step before it
   double ox = 0, oy = 0, oz = 0;
-  for (long long step = 0;; step++) {
-    e = ray_potential(m, charged, ds, px, py, pz);
-    if ((e + minKin) * sl < 0) {
-      if (mag3(qx, qy, qz) > mag3(px, py, pz)) { ox = qx; oy = qy; oz = qz; }
-      else { ox = px; oy = py; oz = pz; }
-      break;
-    } else if ((startX == 0 && startY / py <= 0) || (startY == 0 && startX / px <= 0) ||
-               (startX / px <= 0 && startY / py <= 0)) {
+  for (long long s0 = 0;; s0 += 32) {
+    double px = bx, py = by, pz = bz;
+    for (int k = 0; k < lane; k++) { px = px + vxs; py = py + vys; pz = pz + vzs; }
+    const double e = ray_potential(m, charged, ds, px, py, pz);
+    const bool stop_e = (e + minKin) * sl < 0;
+    const bool stop_axis = (startX == 0 && startY / py <= 0) ||
+                           (startY == 0 && startX / px <= 0) ||
+                           (startX / px <= 0 && startY / py <= 0);
+    // prevPos of each lane's step: the lane below, or the previous chunk's last
+    double rx = __shfl_up_sync(0xffffffffu, px, 1), ry = __shfl_up_sync(0xffffffffu, py, 1),
+           rz = __shfl_up_sync(0xffffffffu, pz, 1);
+    if (lane == 0) { rx = qx; ry = qy; rz = qz; }
+    const unsigned stops = __ballot_sync(0xffffffffu, stop_e || stop_axis);
+    if (stops) {
+      const int f = __ffs(stops) - 1;               // the serial march's stopping step
+      if (lane == f && stop_e) {
+        if (mag3(rx, ry, rz) > mag3(px, py, pz)) { ox = rx; oy = ry; oz = rz; }
+        else { ox = px; oy = py; oz = pz; }
+      }
+      ox = __shfl_sync(0xffffffffu, ox, f);
+      oy = __shfl_sync(0xffffffffu, oy, f);
+      oz = __shfl_sync(0xffffffffu, oz, f);
       break;
     }
-    qx = px; qy = py; qz = pz;
-    px = px + vxs; py = py + vys; pz = pz + vzs;
-    if (step > kMaxSteps) { atomicExch(err, 1); break; }
+    qx = __shfl_sync(0xffffffffu, px, 31);
+    qy = __shfl_sync(0xffffffffu, py, 31);
+    qz = __shfl_sync(0xffffffffu, pz, 31);
+    bx = qx + vxs; by = qy + vys; bz = qz + vzs;
+    if (s0 > kMaxSteps) {
+      if (lane == 0) atomicExch(err, 1);
+      break;
+    }
   }
-  out[3 * r] = ox;
-  out[3 * r + 1] = oy;
-  out[3 * r + 2] = oz;
+  if (lane == 0) {
+    out[3 * r] = ox;
+    out[3 * r + 1] = oy;
+    out[3 * r + 2] = oz;
+  }
 }
 
 namespace host {
@@ -117,8 +146,8 @@ int boundary_march_gpu(int device, int n_atoms, const double *x, const double *y
   if (e == cudaSuccess) {
     RayAtoms m{d_atoms, d_atoms + na, d_atoms + 2 * na, d_atoms + 3 * na, d_atoms + 4 * na,
                d_atoms + 5 * na, n_atoms};
-    const int block = 8;   // few threads per CTA: the rays spread over all SMs
-    const int grid = (int)((nr + block - 1) / block);
+    const int block = 64;  // two rays (warps) per CTA: the rays spread over all SMs
+    const int grid = (int)((nr * 32 + block - 1) / block);
     boundary_rays<<<grid, block>>>(m, charged, dipole_scalar, min_kin, z_max, z_inc, levels,
                                    rotations, d_dirs, d_dirs + rotations, d_dirs + 2 * rotations,
                                    d_dirs + 3 * rotations, d_out, d_err);
