@@ -38,8 +38,10 @@ N_TRAJ = 100_000
 SEED = 20251203
 # Algorithmic FP32 work per pair term, from the reference's formulas
 # (forceAccel.cpp:856-884 LJ; :751-805 LJ + charge field and gradient):
-# flops with FMA = 2, division and square root = 1.
+# flops with FMA = 2, division and square root = 1.  A charge-field pair
+# outside the LJ cut-off (variants 1-3) skips the LJ term's 14 flops.
 FLOPS_LJ, FLOPS_ES, FLOPS_FAR = 22, 55, 60
+FLOPS_ES_NOLJ = 41
 FLOPS_POT_CHARGED, FLOPS_POT_NEUTRAL = 24, 15
 
 
@@ -190,8 +192,8 @@ def roofline_traffic():
 def flops_of(s, charged: bool) -> float:
     """Algorithmic flops of a work record (pair terms by kind)."""
     pot = FLOPS_POT_CHARGED if charged else FLOPS_POT_NEUTRAL
-    return (FLOPS_LJ * s.pair_lj + FLOPS_ES * s.pair_es + FLOPS_FAR * s.far_terms +
-            pot * s.pair_pot)
+    return (FLOPS_LJ * s.pair_lj + FLOPS_ES * (s.pair_es - s.pair_es_nolj) +
+            FLOPS_ES_NOLJ * s.pair_es_nolj + FLOPS_FAR * s.far_terms + pot * s.pair_pot)
 
 
 def autotune(ctx, stream, torch, d_sums) -> int:
@@ -246,7 +248,7 @@ def profile_case(args, mol, par, stream, torch) -> None:
             ctx.set_handoff(args.profile_budget, 0)
         n = args.profile_traj
         m = max(1, args.profile_integrals)
-        d_many = torch.zeros((m + 1) * 128, dtype=torch.uint8, device="cuda")
+        d_many = torch.zeros((m + 1) * abi.C.sizeof(abi.CcsSums), dtype=torch.uint8, device="cuda")
         for k in range(args.warmup + args.steps):
             if m == 1:
                 ctx.run_sampled_device(SEED, k * n, n, 0, d_sums.data_ptr(), stream)
@@ -678,9 +680,7 @@ def molecule_workload(args, rank, world, local, dist, torch):
     kmean = ctx.kernel_ms() / args.steps if args.steps * n_traj <= (1 << 22) else call_ms / args.steps
     mean_ms = shard.max_over_ranks(call_ms / args.steps, dist, "cuda")
     value = world * n_traj / (mean_ms / 1000.0)
-    pot_flops = FLOPS_POT_CHARGED if par.charged else FLOPS_POT_NEUTRAL
-    achieved = (FLOPS_LJ * work.pair_lj + FLOPS_ES * work.pair_es + FLOPS_FAR * work.far_terms +
-                pot_flops * work.pair_pot) / args.steps / (kmean / 1000.0) / 1e12
+    achieved = flops_of(work, bool(par.charged)) / args.steps / (kmean / 1000.0) / 1e12
     fp32_peak, fp64_peak = engine.probe_peaks(local)
     peak = fp32_peak if form == abi.MIXED else fp64_peak
     merged = shard.merge_sums(sums, dist, "cuda")

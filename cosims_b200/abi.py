@@ -11,7 +11,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK, ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_IO, ERR_TIMEOUT, ERR_UNSUPPORTED, ERR_BUSY = range(8)
 
@@ -72,7 +72,8 @@ class CcsSums(C.Structure):
                 ("n", C.c_int64), ("n_hit", C.c_int64), ("n_success", C.c_int64),
                 ("n_eff", C.c_int64), ("steps", C.c_int64), ("force_evals", C.c_int64),
                 ("pot_evals", C.c_int64), ("pair_lj", C.c_int64), ("pair_es", C.c_int64),
-                ("pair_pot", C.c_int64), ("far_terms", C.c_int64)]
+                ("pair_pot", C.c_int64), ("far_terms", C.c_int64),
+                ("pair_es_nolj", C.c_int64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -485,6 +485,7 @@ cosims_status cosims_batch_counters(cosims_batch *b, cosims_ccs_sums *work, floa
   work->pair_es = (int64_t)c[C_PAIR_ES];
   work->pair_pot = (int64_t)c[C_PAIR_POT];
   work->far_terms = (int64_t)c[C_FAR];
+  work->pair_es_nolj = (int64_t)c[C_PAIR_ESNL];
   if (ms) {
     e = cudaEventElapsedTime(ms, b->ev0, b->ev1);
     if (e != cudaSuccess) return cuda_fail(e, "batch timing");

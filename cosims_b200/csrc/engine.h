@@ -137,6 +137,7 @@ enum Counter : int {
   C_PAIR_ES,        // electrostatic (+LJ) pair terms
   C_PAIR_POT,       // potential pair terms
   C_FAR,            // far-field cluster terms
+  C_PAIR_ESNL,      // electrostatic pair terms outside the LJ cut-off (no LJ term)
   C_ERROR,          // error flags (bit 0: staging wait gave up; bit 1: hand-off wait gave up)
   C_T_START_INV,    // ~(earliest CTA start), globaltimer ns (max of complements)
   C_T_DRAIN_INV,    // ~(first time a group found the work queue empty)

@@ -385,7 +385,10 @@ __device__ __forceinline__ void far_values(const Far2 &t, float (&v)[12]) {
   v[9] = t.Maxy.x + t.Maxy.y; v[10] = t.Maxz.x + t.Maxz.y; v[11] = t.Mayz.x + t.Mayz.y;
 }
 
-struct WorkM { uint32_t lj, es, far; };
+// Pair counters of one evaluation: LJ-only, charge-field (+ LJ inside the
+// cut-off) and far-field terms, and nl: charge-field pairs outside the LJ
+// cut-off (no LJ term, fewer flops).
+struct WorkM { uint32_t lj, es, far, nl; };
 
 // Reduce-scatter of K values over a group of G lanes (G a power of two <= 32,
 // aligned in the warp) by recursive halving: at each level a lane keeps half
@@ -498,6 +501,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
         in = !(d0 * d0 + d1 * d1 + d2 * d2 > C.dr2);
         if (TYPE == 5 && in) w.lj += (uint32_t)C.n_atoms;
+        if (TYPE == 3 && !in) w.nl += (uint32_t)C.n_atoms;
         fac[c] = in ? 1.0f : 0.0f;
       }
       const unsigned b = __ballot_sync(0xffffffffu, in);
@@ -562,6 +566,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         const uint32_t cnt = (uint32_t)C.n_atoms;
         if (mode & M_ES) w.es += cnt;
         else if (mode) w.lj += cnt;
+        if ((mode & M_ES) && !(mode & M_LJ)) w.nl += cnt;
         fx = (float)d0; fy = (float)d1; fz = (float)d2;
       }
       const bool es = (mode & M_ES) != 0, ljo = mode != 0 && !es;
@@ -681,6 +686,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         if (mode & M_ES) w.es += cnt;
         else if (mode) w.lj += cnt;
       }
+      if ((mode & M_ES) && !(mode & M_LJ)) w.nl += (uint32_t)C.n_atoms;
     }
     ln.sync();
     // pass 2: atom slots, two per lane per pass (G <= 32 and slots come in
@@ -852,7 +858,7 @@ static_assert(sizeof(GroupState) == kGroupStateBytes, "GroupState layout");
 // Pair counters of one lane (force variants 1, 2, 5), added to the group's
 // counters once the lane is done.
 struct Tally {
-  uint32_t lj = 0, es = 0, far = 0;
+  uint32_t lj = 0, es = 0, far = 0, nl = 0;
 };
 
 __device__ __forceinline__ void group_counters_clear(GroupState &G) {
@@ -860,6 +866,12 @@ __device__ __forceinline__ void group_counters_clear(GroupState &G) {
 }
 
 // Fold a lane's pair tally into its group (shared-memory atomics, once).
+// A lane's charge-only pair count goes straight to the global counter (every
+// lane, once, at the end of its narrow phase).
+__device__ __forceinline__ void flush_nolj(const Tally &tl, unsigned long long *c) {
+  count_add(c, C_PAIR_ESNL, tl.nl);
+}
+
 template <int TYPE>
 __device__ __forceinline__ void fold_tally(GroupState &G, const Tally &tl) {
   if (Traits<TYPE>::kVaryingPairs) {
@@ -1036,10 +1048,13 @@ __device__ __forceinline__ void group_loop(const View &m, const View64 &m64, con
     ln.sync();
 
     double an[3];
-    WorkM wi = {0, 0, 0};
+    WorkM wi = {0, 0, 0, 0};
     force<TYPE, PackedFar<Src>::value>(m, p, ep, an, ln, modes, wi);
     if (Traits<TYPE>::kVaryingPairs) {
       tl.lj += wi.lj; tl.es += wi.es; tl.far += wi.far;
+    }
+    if (Traits<TYPE>::kCharge && Traits<TYPE>::kClusters) {
+      tl.nl += wi.nl;
     }
     double U = 0;
     if (ln.any(needU)) {
@@ -1267,6 +1282,7 @@ __device__ __forceinline__ void wide_force(const View &m, const DevParams &p, co
         if (mode & M_ES) tl.es += cnt;
         else if (mode) tl.lj += cnt;
       }
+      if ((mode & M_ES) && !(mode & M_LJ)) tl.nl += (uint32_t)C.n_atoms;
     }
     wd.sync();
     int k = lane;
@@ -1576,6 +1592,7 @@ __device__ __noinline__ void wide_phase(unsigned char *smem, uint32_t img_bytes,
     count_add(counters, C_PAIR_ES, tl.es);
     count_add(counters, C_FAR, tl.far);
   }
+  count_add(counters, C_PAIR_ESNL, tl.nl);
   if (wd.lane == 0) {
     count_add(counters, C_WIDE_STEPS, (long long)nsteps);
     count_add(counters, C_WIDE_NS, (long long)(global_ns() - t0));
@@ -1640,6 +1657,7 @@ __global__ void __launch_bounds__(KernelShape<TYPE>::kMaxThreads, COSIMS_MIXED_M
   Tally tl;
   group_loop<TYPE>(m, m64, a.par, ln, modes, *S, src, tl);
   fold_tally<TYPE>(*S, tl);
+  flush_nolj(tl, a.counters);
   __syncwarp();
   if (ln.lane == 0) flush_group<TYPE>(*S, m64.n, a.counters);
   if (a.ho.budget > 0) {

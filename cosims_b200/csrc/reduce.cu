@@ -148,6 +148,7 @@ __global__ void reduce_final(const cosims_traj_out *__restrict__ recs, long long
     s.pair_es = counters ? (int64_t)counters[C_PAIR_ES] : 0;
     s.pair_pot = counters ? (int64_t)counters[C_PAIR_POT] : 0;
     s.far_terms = counters ? (int64_t)counters[C_FAR] : 0;
+    s.pair_es_nolj = counters ? (int64_t)counters[C_PAIR_ESNL] : 0;
     *out = s;
   }
 }
@@ -165,6 +166,7 @@ __global__ void add_work_kernel(const unsigned long long *counters, cosims_ccs_s
   w->pair_es += (int64_t)counters[C_PAIR_ES];
   w->pair_pot += (int64_t)counters[C_PAIR_POT];
   w->far_terms += (int64_t)counters[C_FAR];
+  w->pair_es_nolj += (int64_t)counters[C_PAIR_ESNL];
 }
 
 int add_work_launch(const unsigned long long *counters, cosims_ccs_sums *d_work, int zero_first,

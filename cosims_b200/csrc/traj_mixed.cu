@@ -121,6 +121,7 @@ __device__ __noinline__ void batch_session(const BatchMol &bm, unsigned char *sm
   Tally tl;
   group_loop<TYPE>(m, m64, bm.par, ln, modes, *S, src, tl);
   fold_tally<TYPE>(*S, tl);
+  flush_nolj(tl, a.counters);
   __syncwarp();
   if (ln.lane == 0) flush_group<TYPE>(*S, m64.n, a.counters);
 }

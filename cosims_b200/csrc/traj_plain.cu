@@ -39,6 +39,7 @@ __device__ __forceinline__ View make_view(const unsigned char *base, const MolIm
 
 struct Work {          // per-thread work counters, flushed when a trajectory ends
   uint32_t lj, es, pot, far;
+  uint32_t nl;         // of es: outside the LJ cut-off (charge field only)
 };
 
 // multipoleCutoff (type 1, forceAccel.cpp:221-445) / multipoleOnly (type 2,
@@ -164,6 +165,7 @@ __device__ void force_multipole(const View &m, const DevParams &p, const double 
         }
       }
       w.es += a1 - a0;
+      if (!lj) w.nl += a1 - a0;
     }
   }
   const double ds = p.dipole_scalar;
@@ -214,6 +216,7 @@ __device__ void force_dispersion_only(const View &m, const DevParams &p, const d
       }
     }
     w.es += a1 - a0;
+    if (!lj) w.nl += a1 - a0;
   }
   const double ds = p.dipole_scalar;
   sumX += ds * (diagMatXX * fieldX + sMatXY * fieldY + sMatXZ * fieldZ);
@@ -628,6 +631,7 @@ __device__ __forceinline__ void event_terms(const View &m, const DevParams &p, c
     o.put(ljk + 2, 0, scalarComp * ex2);
   }
   w.es++;
+  if (!lj) w.nl++;
 }
 
 // The acceleration of the serial force functions, by the whole CTA.
@@ -751,7 +755,7 @@ __device__ void exact_phase(const View &m, const TrajArgs &a, const Exact &x) {
   const DevParams &p = a.par;
   const Handoff &ho = a.ho;
   const long long cap = p.max_steps > 0 ? p.max_steps : kDefaultMaxSteps;
-  Work w = {0, 0, 0, 0};
+  Work w = {0, 0, 0, 0, 0};
   uint32_t nforce = 0, npot = 0;
   unsigned long long nsteps = 0;
   const unsigned long long t0 = global_ns();
@@ -860,6 +864,7 @@ __device__ void exact_phase(const View &m, const TrajArgs &a, const Exact &x) {
   count_add(c, C_PAIR_LJ, w.lj);
   count_add(c, C_PAIR_ES, w.es);
   count_add(c, C_FAR, w.far);
+  count_add(c, C_PAIR_ESNL, w.nl);
   if (threadIdx.x == 0) {
     count_add(c, C_STEPS, (long long)nsteps);
     count_add(c, C_FORCE_EVALS, nforce);
@@ -907,7 +912,7 @@ __global__ void __launch_bounds__(kPlainBlock, PlainShape<TYPE>::kMinBlocks)
   int orbits = 0, step = 0, phase = P_ACQUIRE;
   long long total = 0, t = 0;
   unsigned etries = 0, otries = 0;
-  Work w = {0, 0, 0, 0};
+  Work w = {0, 0, 0, 0, 0};
   uint32_t nforce = 0, npot = 0;
   unsigned long long nsteps = 0;
 
@@ -964,13 +969,13 @@ __global__ void __launch_bounds__(kPlainBlock, PlainShape<TYPE>::kMinBlocks)
     }
 
     double an[3];
-    Work wi = {0, 0, 0, 0};
+    Work wi = {0, 0, 0, 0, 0};
     force<TYPE>(m, p, ep, an, wi);
     double U = 0;
     if (__any_sync(0xffffffffu, needU)) U = potential(m, p, ep);
     if (phase == P_DONE) continue;
     nforce++;
-    w.lj += wi.lj; w.es += wi.es; w.far += wi.far;
+    w.lj += wi.lj; w.es += wi.es; w.far += wi.far; w.nl += wi.nl;
     if (needU) { npot++; w.pot += m.n; }
 
     if (phase == P_INIT_FIRST || phase == P_INIT_RETRY) {
@@ -1055,6 +1060,7 @@ __global__ void __launch_bounds__(kPlainBlock, PlainShape<TYPE>::kMinBlocks)
   count_add(c, C_PAIR_ES, w.es);
   count_add(c, C_PAIR_POT, w.pot);
   count_add(c, C_FAR, w.far);
+  count_add(c, C_PAIR_ESNL, w.nl);
   if (!TRACE && a.ho.budget > 0) {
     __syncthreads();                    // every thread done: the CTA goes wide
     const Exact x = exact_scratch(smem, a.use_smem ? a.img.bytes : 0u, TYPE, m.nc);

@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define COSIMS_ABI_VERSION 1
+#define COSIMS_ABI_VERSION 2
 
 typedef enum cosims_status {
     COSIMS_OK = 0,
@@ -158,6 +158,8 @@ typedef struct cosims_ccs_sums {
     int64_t pair_es;      /* pair terms with the charge field (+ LJ if in range) */
     int64_t pair_pot;     /* potential pair terms (energy check)                 */
     int64_t far_terms;    /* cluster multipole far-field terms                   */
+    int64_t pair_es_nolj; /* of pair_es, those outside the LJ cut-off: the charge
+                             field and its gradient only (force variants 1-3)   */
 } cosims_ccs_sums;
 
 typedef struct cosims_ctx cosims_ctx;

@@ -35,7 +35,7 @@ def test_abi_version_and_layouts():
     L = engine.lib()
     assert L.cosims_abi_version() == abi.ABI_VERSION
     assert C.sizeof(abi.TrajOut) == 24 and C.sizeof(abi.TrajIn) == 40
-    assert C.sizeof(abi.CcsSums) == 14 * 8
+    assert C.sizeof(abi.CcsSums) == 15 * 8
 
 
 def test_device_calls_fail_cleanly_without_a_gpu():

@@ -109,6 +109,7 @@ def test_run_integrals_equals_separate_integrals(name, precision):
     assert work.steps == sum(b.steps for b in sep)
     assert work.force_evals == sum(b.force_evals for b in sep)
     assert work.pair_lj + work.pair_es == sum(b.pair_lj + b.pair_es for b in sep)
+    assert work.pair_es_nolj == sum(b.pair_es_nolj for b in sep)
     assert work.sum == 0 and work.n == 0
 
 
@@ -134,3 +135,22 @@ def test_reserve_allocates_before_the_calls(precision):
             ctx.reserve(-1, 1)
     for a, b in zip(got, want):
         assert (a.sum, a.sum2, a.n_hit, a.n_eff) == (b.sum, b.sum2, b.n_hit, b.n_eff)
+
+
+@pytest.mark.parametrize("precision", [abi.PLAIN_F64, abi.MIXED])
+def test_charge_only_pairs_counted(precision):
+    """pair_es_nolj: the charge-field pairs outside the LJ cut-off (variant 3's
+    clusters beyond the dispersion radius), a subset of pair_es; none for the
+    neutral variant 5.  Both forms count the same clusters, so on the same
+    sampled trajectories their shares agree closely."""
+    shares = {}
+    for name in ("c1_t3", "c0_t5"):
+        mol, par, _ = load(name)
+        with engine.Context(mol, par, precision) as ctx:
+            s, _, _ = ctx.run_sampled(seed=3, first=0, n=2000)
+        if name == "c0_t5":
+            assert s.pair_es_nolj == 0
+        else:
+            assert 0 < s.pair_es_nolj < s.pair_es
+            shares[name] = s.pair_es_nolj / s.pair_es
+    assert 0.2 < shares["c1_t3"] < 0.95
