@@ -1050,10 +1050,13 @@ __device__ __forceinline__ void group_loop(const View &m, const View64 &m64, con
     double an[3];
     WorkM wi = {0, 0, 0, 0};
     force<TYPE, PackedFar<Src>::value>(m, p, ep, an, ln, modes, wi);
-    if (Traits<TYPE>::kVaryingPairs) {
+    // a group without a trajectory evaluates at a dummy point only to keep the
+    // warp's shuffles convergent: its pair terms are not counted (their number
+    // depends on when the other groups of the warp finish)
+    if (Traits<TYPE>::kVaryingPairs && phase != P_DONE) {
       tl.lj += wi.lj; tl.es += wi.es; tl.far += wi.far;
     }
-    if (Traits<TYPE>::kCharge && Traits<TYPE>::kClusters) {
+    if (Traits<TYPE>::kCharge && Traits<TYPE>::kClusters && phase != P_DONE) {
       tl.nl += wi.nl;
     }
     double U = 0;
