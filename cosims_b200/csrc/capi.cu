@@ -287,6 +287,41 @@ void build_images(const cosims_molecule *m, const cosims_params *p, HostImage &h
     i32.off[S_LJ] = b32.add(b4.data(), sizeof(float4) * ns);
   }
   i32.off[S_CLUSTERS] = b32.add(c32.data(), sizeof(ClusterF32) * (nc + 1));
+  if (p->force_type == 1 || p->force_type == 2) {
+    // far-field table: clusters 2j, 2j+1 side by side (see engine.h)
+    const int nfp = far_table_pairs(nc);
+    std::vector<float4> ft((size_t)kFarTableArrays * nfp);
+    for (int j = 0; j < nfp; j++) {
+      // per cluster: -x_hi, -y_hi, -z_hi, -x_lo, -y_lo, -z_lo, mpr2, dr2, q, dipole;
+      // a null entry sits 1e4 A out with zero moments and radii -1
+      float v[12][2];
+      for (int h = 0; h < 2; h++) {
+        const int c = 2 * j + h;
+        float w[12] = {-1.0e4f, -1.0e4f, -1.0e4f, 0.0f, 0.0f, 0.0f, -1.0f, -1.0f,
+                       0.0f, 0.0f, 0.0f, 0.0f};
+        if (c < nc) {
+          const ClusterF32 &F = c32[c];
+          const double ctr[3] = {F.cx, F.cy, F.cz};
+          for (int k = 0; k < 3; k++) {
+            const float hi = (float)ctr[k];
+            w[k] = -hi;
+            w[3 + k] = -(float)(ctr[k] - (double)hi);
+          }
+          w[6] = (float)F.mpr2;
+          w[7] = (float)F.dr2;
+          w[8] = F.q;
+          for (int k = 0; k < 3; k++) w[9 + k] = F.dip[k];
+        }
+        for (int k = 0; k < 12; k++) v[k][h] = w[k];
+      }
+      // value pairs (2a, 2a+1) of the two clusters in array a:
+      // (x_hi, y_hi), (z_hi, x_lo), (y_lo, z_lo), (mpr2, dr2), (q, dip_x), (dip_y, dip_z)
+      for (int a = 0; a < kFarTableArrays; a++)
+        ft[(size_t)a * nfp + j] = make_float4(v[2 * a][0], v[2 * a][1], v[2 * a + 1][0],
+                                              v[2 * a + 1][1]);
+    }
+    i32.off[S_FAR] = b32.add(ft.data(), sizeof(float4) * ft.size());
+  }
   b32.finish();
   i32.bytes = (uint32_t)b32.buf.size();
   i32.n_atoms = n;
@@ -371,6 +406,8 @@ cosims_status shape_for(bool plain, const MolImage &img, int G, int block_thread
   if (!plain && block_threads == 0) {
     cands[0] = 256; cands[1] = 512; cands[2] = kMixedMaxBlock;
     ncand = 3;
+    // variants 1 and 2 run at most kMixedFarBlock threads (96 registers)
+    if (force_type == 1 || force_type == 2) cands[ncand++] = kMixedFarBlock;
   }
   bool found = false;
   int best_resident = -1;
@@ -416,14 +453,19 @@ cosims_status shape_for(bool plain, const MolImage &img, int G, int block_thread
       // groups from shared memory); plain form: every lane of a warp reads the
       // same atom, a broadcast that L1 serves as well, so the most resident
       // threads win (the staged shape on a tie)
-      const int resident = per_sm * block * (t.use_smem && !plain ? 2 : 1);
+      // a shape that keeps the requested long-trajectory hand-off beats one
+      // that drops it (a CTA shrunk below the wide group size has none)
+      const bool keeps_wide = !per_wide || t.wide_lanes > 0;
+      const int resident = per_sm * block * (t.use_smem && !plain ? 2 : 1) +
+                           (keeps_wide ? (1 << 24) : 0);
       if (resident > best_resident) {
         best_resident = resident;
         t.grid = per_sm;                // CTAs per SM until the grid is sized below
         ls = t;
         found = true;
       }
-      if (per_sm > 0 && !plain) break;  // staged works: no need to try unstaged
+      // staged works: no need to try unstaged, unless staging dropped the hand-off
+      if (per_sm > 0 && !plain && keeps_wide) break;
     }
   }
   if (!found) return fail(COSIMS_ERR_UNSUPPORTED, "molecule image does not fit in shared memory");

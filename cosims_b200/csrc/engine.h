@@ -37,6 +37,13 @@
 //     24 eps/mu 0, 24 eps/mu 1) and the two cluster ids.  A lane's float4 load
 //     then yields the register pairs that Blackwell's packed FP32 instructions
 //     (FFMA2 and kin) take, with no moves to assemble them.
+//     Variants 1 and 2 also hold the far-field table (S_FAR): clusters 2j and
+//     2j+1 side by side in six float4 arrays over j, for the packed far pass:
+//     the negated centre as an FP32 hi/lo pair (-x_hi, -y_hi, -z_hi, then
+//     -x_lo, -y_lo, -z_lo), the squared multipole and dispersion radii in FP32,
+//     the charge and the dipole (0 for a replaced cluster).  Pairs past the
+//     last cluster are null entries (zero moments, radii -1: far, never in the
+//     dispersion radius); the table has a multiple of kMaxGroupLanes pairs.
 #pragma once
 #include <cstdint>
 #include "cosims_cuda.h"
@@ -56,13 +63,18 @@ __host__ __device__ constexpr bool blocked_layout(int force_type) {
 }
 constexpr float kPadCoord = 1.0e6f;                // pad atoms sit this far out (Angstrom)
 constexpr int kMixedMaxBlock = 768;                // threads per CTA of the mixed kernels (80 registers)
-constexpr int kMixedFarBlock = 512;                // variants 1, 2: 128 registers for the far field
+constexpr int kMixedFarBlock = 640;                // variants 1, 2: 96 registers, 20 warps a CTA
 constexpr int kBatchMaxBlock = 512;                // threads per CTA of the batched kernel
 constexpr int kTrajStateBytes = 200;               // one trajectory's integrator state
 constexpr int kGroupStateBytes = 240;              // TrajState + a group's counters (shared memory)
 constexpr int kWideSlotFloats = 24;                // per-warp reduction slot of a wide group
 
-enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_LJ, S_SLOTS, S_PAIRS, S_COUNT };
+enum ImageSection : int { S_ATOMS = 0, S_PERM, S_CLUSTERS, S_LJ, S_SLOTS, S_PAIRS, S_FAR, S_COUNT };
+// far-field table of variants 1 and 2: pairs of clusters, six float4 per pair
+__host__ __device__ constexpr int far_table_pairs(int n_clusters) {
+  return ((n_clusters + 1) / 2 + kMaxGroupLanes - 1) / kMaxGroupLanes * kMaxGroupLanes;
+}
+constexpr int kFarTableArrays = 6;
 // variants whose F32 image is pair-interleaved (S_PAIRS instead of S_ATOMS / S_LJ)
 __host__ __device__ constexpr bool paired_layout(int force_type) {
   return force_type == 3 || force_type == 4 || force_type == 6;

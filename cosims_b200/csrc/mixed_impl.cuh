@@ -36,7 +36,9 @@ struct View {
   const float4 *pl;        // sigma^6 0, sigma^6 1, 24 eps/mu 0, 24 eps/mu 1
   const uint2 *pc;         // cluster ids
   const ClusterF32 *cl;
+  const float4 *ft;        // far-field table (variants 1, 2): clusters 2j, 2j+1 per entry j
   int n, nc, nslots;        // atoms, clusters, padded atom slots
+  int nfp;                  // far-field table pairs (a multiple of 32)
 };
 
 struct View64 {   // FP64 image in global memory, for the energy check
@@ -54,9 +56,11 @@ __device__ __forceinline__ View make_view(const unsigned char *b, const MolImage
   v.pl = v.pz + np;
   v.pc = reinterpret_cast<const uint2 *>(v.pl + np);
   v.cl = reinterpret_cast<const ClusterF32 *>(b + img.off[S_CLUSTERS]);
+  v.ft = reinterpret_cast<const float4 *>(b + img.off[S_FAR]);
   v.n = img.n_atoms;
   v.nc = img.n_clusters;
   v.nslots = img.n_slots;
+  v.nfp = far_table_pairs(img.n_clusters);
   return v;
 }
 
@@ -301,18 +305,21 @@ __device__ __forceinline__ float2 neg2(const float2 &a) { return f2(-a.x, -a.y);
 // as in far_terms).  Replaced clusters carry a zero dipole in the F32 image;
 // the null cluster (index n_clusters, zero moments) adds exactly 0 at any
 // finite distance, so it fills a half that has no far cluster.
-__device__ __forceinline__ void far2(const View &m, int ia, int ib, int order, const float2 &dx,
-                                     const float2 &dy, const float2 &dz, Far2 &s) {
-  const ClusterF32 &A = m.cl[ia];
-  const ClusterF32 &B = m.cl[ib];
-  const float2 xx = __fmul2_rn(dx, dx), yy = __fmul2_rn(dy, dy), zz = __fmul2_rn(dz, dz);
-  const float2 r2 = __fadd2_rn(__fadd2_rn(xx, yy), zz);
-  const float2 r_1 = f2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+//
+// far2_core takes the two clusters' separations, their squares, r2 and 1/r,
+// charges, dipoles and (order 2) quadrupoles.  Every term carries a power of
+// 1/r, so a half whose 1/r is 0 adds exactly 0 (with finite separations).
+__device__ __forceinline__ void far2_core(int order, const float2 &dx, const float2 &dy,
+                                          const float2 &dz, const float2 &xx, const float2 &yy,
+                                          const float2 &zz, const float2 &r2, const float2 &r_1,
+                                          const float2 &q, const float2 &D0, const float2 &D1,
+                                          const float2 &D2, const float *QA, const float *QB,
+                                          Far2 &s) {
   const float2 r_2 = __fmul2_rn(r_1, r_1);
   const float2 r_3 = __fmul2_rn(r_2, r_1);
   const float2 r_5 = __fmul2_rn(r_3, r_2);
   const float2 xy = __fmul2_rn(dx, dy), xz = __fmul2_rn(dx, dz), yz = __fmul2_rn(dy, dz);
-  const float2 cR5 = __fmul2_rn(f2(A.q, B.q), r_5);
+  const float2 cR5 = __fmul2_rn(q, r_5);
   const float2 cR3 = __fmul2_rn(cR5, r2);
   const float2 m3 = f2(-3.0f, -3.0f);
   s.Ex = __ffma2_rn(cR3, dx, s.Ex);
@@ -325,8 +332,6 @@ __device__ __forceinline__ void far2(const View &m, int ia, int ib, int order, c
   s.Msxz = __ffma2_rn(__fmul2_rn(m3, xz), cR5, s.Msxz);
   s.Msyz = __ffma2_rn(__fmul2_rn(m3, yz), cR5, s.Msyz);
   if (order >= 1) {
-    const float2 D0 = f2(A.dip[0], B.dip[0]), D1 = f2(A.dip[1], B.dip[1]),
-                 D2 = f2(A.dip[2], B.dip[2]);
     const float2 r_7 = __fmul2_rn(r_5, r_2);
     const float2 c1 = __fmul2_rn(f2(3.0f, 3.0f),
                                  __ffma2_rn(D2, dz, __ffma2_rn(D1, dy, __fmul2_rn(D0, dx))));
@@ -348,7 +353,6 @@ __device__ __forceinline__ void far2(const View &m, int ia, int ib, int order, c
     s.Mayz = __ffma2_rn(__ffma2_rn(D2, dy, __fmul2_rn(neg2(D1), dz)), r5_3, s.Mayz);
   }
   if (order >= 2) {
-    const float *QA = A.quad, *QB = B.quad;
     const float2 r_7 = __fmul2_rn(r_5, r_2);
     const float2 t0 = __fmul2_rn(__ffma2_rn(f2(QA[6], QB[6]), dz,
                                   __ffma2_rn(f2(QA[3], QB[3]), dy, __fmul2_rn(f2(QA[0], QB[0]), dx))), r_7);
@@ -374,6 +378,17 @@ __device__ __forceinline__ void far2(const View &m, int ia, int ib, int order, c
     s.Maxz = __ffma2_rn(p5, __ffma2_rn(t2, dx, __fmul2_rn(neg2(t0), dz)), s.Maxz);
     s.Mayz = __ffma2_rn(p5, __ffma2_rn(t2, dy, __fmul2_rn(neg2(t1), dz)), s.Mayz);
   }
+}
+
+__device__ __forceinline__ void far2(const View &m, int ia, int ib, int order, const float2 &dx,
+                                     const float2 &dy, const float2 &dz, Far2 &s) {
+  const ClusterF32 &A = m.cl[ia];
+  const ClusterF32 &B = m.cl[ib];
+  const float2 xx = __fmul2_rn(dx, dx), yy = __fmul2_rn(dy, dy), zz = __fmul2_rn(dz, dz);
+  const float2 r2 = __fadd2_rn(__fadd2_rn(xx, yy), zz);
+  const float2 r_1 = f2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
+  far2_core(order, dx, dy, dz, xx, yy, zz, r2, r_1, f2(A.q, B.q), f2(A.dip[0], B.dip[0]),
+            f2(A.dip[1], B.dip[1]), f2(A.dip[2], B.dip[2]), A.quad, B.quad, s);
 }
 
 // The 12 far-field sums of a lane (both halves added), in the order of the
@@ -543,6 +558,8 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     const unsigned gbits = G == 32 ? 0xffffffffu : ((1u << G) - 1u);
     const unsigned below = (1u << lane) - 1u;
     int n_es = 0, n_lj = 0;
+    // the far-table pass leaves the pair counts of the listed clusters to pass 2
+    bool count_listed = false;
     // one round: the clusters c0 + lane; returns whether the lane's cluster
     // is far, with its distance rounded to FP32
     auto classify = [&](int c0, float &fx, float &fy, float &fz) {
@@ -580,23 +597,88 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
       return far;
     };
     if (Traits<TYPE>::kFar && PACKED_FAR && G >= 16) {
-      // far field in the same pass (variants 1 and 2, G >= 16): two rounds
-      // at a time, the lane's far cluster of each in one half of the packed
-      // instructions (the null cluster fills a half without one).  The 12
-      // sums are reduced over the group at once (reduce-scatter: one value
-      // per lane), so the pair loop below runs with one extra register
-      // instead of 24.
+      // far field in the same pass (variants 1 and 2, G >= 16), from the
+      // far-field table: lane j of a round takes clusters 2j and 2j+1, one per
+      // half of the packed instructions.  The separations come from the FP32
+      // hi/lo centres and the He position (as accurate as the FP64 difference
+      // rounded to FP32), and the near/far and dispersion tests run on them;
+      // a squared distance within 2^-16 (relative) of a radius is tested again
+      // in FP64 from the cluster record, so every decision is the FP64 test's
+      // (the FP32 value is within about 1e-6 of it).  A near half gets 1/r = 0
+      // and adds exactly 0.  The 12 sums are reduced over the group at once
+      // (reduce-scatter: one value per lane), so the pair loop below runs with
+      // one extra register instead of 24.
       Far2 f = {};
-      for (int c0 = 0; c0 < m.nc; c0 += 2 * G) {
-        float ax = 1.0e4f, ay = 1.0e4f, az = 1.0e4f, bx = 1.0e4f, by = 1.0e4f, bz = 1.0e4f;
-        const bool fa = classify(c0, ax, ay, az);
-        const bool fb = c0 + G < m.nc ? classify(c0 + G, bx, by, bz) : false;
-        if (!fa) ax = ay = az = 1.0e4f;
-        if (!fb) bx = by = bz = 1.0e4f;
-        if (fa || fb)
-          far2(m, fa ? c0 + lane : m.nc, fb ? c0 + G + lane : m.nc, p.multipole_order,
-               f2(ax, bx), f2(ay, by), f2(az, bz), f);
+      const float4 *T = m.ft;
+      const int nfp = m.nfp;
+      const float2 hx2 = f2(hx, hx), hy2 = f2(hy, hy), hz2 = f2(hz, hz);
+      const float2 lx2 = f2(lx, lx), ly2 = f2(ly, ly), lz2 = f2(lz, lz);
+      constexpr float kMargin = 1.0f / 65536.0f;
+      for (int jb = 0; jb < nfp; jb += G) {
+        const int j = jb + lane;
+        const float4 t0 = T[j], t1 = T[nfp + j], t2 = T[2 * nfp + j], t3 = T[3 * nfp + j];
+        const float4 t4 = T[4 * nfp + j], t5 = T[5 * nfp + j];
+        const float2 dx = __fadd2_rn(__fadd2_rn(hx2, f2(t0.x, t0.y)), __fadd2_rn(lx2, f2(t1.z, t1.w)));
+        const float2 dy = __fadd2_rn(__fadd2_rn(hy2, f2(t0.z, t0.w)), __fadd2_rn(ly2, f2(t2.x, t2.y)));
+        const float2 dz = __fadd2_rn(__fadd2_rn(hz2, f2(t1.x, t1.y)), __fadd2_rn(lz2, f2(t2.z, t2.w)));
+        const float2 xx = __fmul2_rn(dx, dx), yy = __fmul2_rn(dy, dy), zz = __fmul2_rn(dz, dz);
+        const float2 r2 = __fadd2_rn(__fadd2_rn(xx, yy), zz);
+        bool far_a = r2.x > t3.x, far_b = r2.y > t3.y;
+        bool in_a = !(r2.x > t3.z), in_b = !(r2.y > t3.w);
+        const bool amb = fabsf(r2.x - t3.x) <= kMargin * t3.x ||
+                         fabsf(r2.y - t3.y) <= kMargin * t3.y ||
+                         fabsf(r2.x - t3.z) <= kMargin * t3.z ||
+                         fabsf(r2.y - t3.w) <= kMargin * t3.w;
+        const int ca = 2 * j, cb = 2 * j + 1;
+        if (ln.any(amb) && amb) {
+          // the FP64 tests of both clusters (null entries are never ambiguous:
+          // their radii are -1)
+          const ClusterF32 &A = m.cl[ca];
+          double d0 = pos[0] - A.cx, d1 = pos[1] - A.cy, d2 = pos[2] - A.cz;
+          double q2 = d0 * d0 + d1 * d1 + d2 * d2;
+          far_a = q2 > A.mpr2;
+          in_a = !(q2 > A.dr2);
+          if (cb < m.nc) {
+            const ClusterF32 &B = m.cl[cb];
+            d0 = pos[0] - B.cx; d1 = pos[1] - B.cy; d2 = pos[2] - B.cz;
+            q2 = d0 * d0 + d1 * d1 + d2 * d2;
+            far_b = q2 > B.mpr2;
+            in_b = !(q2 > B.dr2);
+          }
+        }
+        const float2 r_1 = f2(far_a ? rsqrt_ftz(r2.x) : 0.0f, far_b ? rsqrt_ftz(r2.y) : 0.0f);
+        const int qa = ca < m.nc ? ca : m.nc, qb = cb < m.nc ? cb : m.nc;
+        far2_core(p.multipole_order, dx, dy, dz, xx, yy, zz, r2, r_1, f2(t4.x, t4.y),
+                  f2(t4.z, t4.w), f2(t5.x, t5.y), f2(t5.z, t5.w), m.cl[qa].quad, m.cl[qb].quad, f);
+        // the clusters that add pair terms: a near one (charge field), or a
+        // far one inside the dispersion radius (variant 1: band LJ) or, for
+        // variant 2, every far one; null entries (far, never inside) only
+        // need the bound for variant 2
+        const bool es_a = !far_a, es_b = !far_b;
+        const bool lj_a = far_a && (TYPE == 2 ? ca < m.nc : in_a);
+        const bool lj_b = far_b && (TYPE == 2 ? cb < m.nc : in_b);
+        const uint32_t mode_a = es_a ? (M_ES | ((TYPE == 2 || in_a) ? M_LJ : 0))
+                                     : (TYPE == 2 ? M_LJ : M_LJQ);
+        const uint32_t mode_b = es_b ? (M_ES | ((TYPE == 2 || in_b) ? M_LJ : 0))
+                                     : (TYPE == 2 ? M_LJ : M_LJQ);
+        const unsigned e_a = (__ballot_sync(0xffffffffu, es_a) >> gbase) & gbits;
+        const unsigned e_b = (__ballot_sync(0xffffffffu, es_b) >> gbase) & gbits;
+        const unsigned l_a = (__ballot_sync(0xffffffffu, lj_a) >> gbase) & gbits;
+        const unsigned l_b = (__ballot_sync(0xffffffffu, lj_b) >> gbase) & gbits;
+        // lane order, a before b: charge-field clusters from the front, the
+        // LJ-only ones from the back
+        const int pe = n_es + __popc(e_a & below) + __popc(e_b & below);
+        const int pl = m.nc - 1 - n_lj - __popc(l_a & below) - __popc(l_b & below);
+        if (es_a) list[pe] = ((uint32_t)ca << 8) | mode_a;
+        if (es_b) list[pe + (es_a ? 1 : 0)] = ((uint32_t)cb << 8) | mode_b;
+        if (lj_a) list[pl] = ((uint32_t)ca << 8) | mode_a;
+        if (lj_b) list[pl - (lj_a ? 1 : 0)] = ((uint32_t)cb << 8) | mode_b;
+        n_es += __popc(e_a) + __popc(e_b);
+        n_lj += __popc(l_a) + __popc(l_b);
       }
+      // every cluster that adds no charge field is far (variants 1, 2)
+      if (lane == 0) w.far += (uint32_t)(m.nc - n_es);
+      count_listed = true;
       float fv[12];
       far_values(f, fv);
       int idx;
@@ -634,6 +716,17 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         const ClusterF32 &CA = m.cl[ea >> 8];
         const ClusterF32 &CB = m.cl[eb >> 8];
         const int na = CA.a1 - CA.a0, nb = has_b ? CB.a1 - CB.a0 : 0;
+        if (count_listed && sub == 0) {
+          // one lane per listed cluster: its pair terms by kind
+          const uint32_t ca_n = (uint32_t)CA.n_atoms, cb_n = has_b ? (uint32_t)CB.n_atoms : 0u;
+          if (es) {
+            w.es += ca_n + cb_n;
+            if (!(ea & M_LJ)) w.nl += ca_n;
+            if (!(eb & M_LJ)) w.nl += cb_n;
+          } else {
+            w.lj += ca_n + cb_n;
+          }
+        }
         const int nmax = na > nb ? na : nb;
         for (int k = sub; k < nmax; k += split) {
           const int ka = k < na ? CA.a0 + k : inert0 + (k & (kClusterBlock - 1));

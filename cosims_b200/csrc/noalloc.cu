@@ -42,9 +42,9 @@ namespace {
 
 constexpr size_t kNoallocScratchBytes = 12u << 20;       // 12 MiB per device
 constexpr size_t kCtrlBytes = 4096;                       // queue, counters, order scratch
-// molecule images (F64 + F32): about 100 bytes per atom and at most 820 per
-// cluster (its record and the padding of its last slot block), so every
-// molecule of the 16384-atom limit fits with up to 3000 clusters
+// molecule images (F64 + F32): about 100 bytes per atom and at most 850 per
+// cluster (its records, far-field table entry and the padding of its last slot
+// block), so every molecule of the 16384-atom limit fits with up to 3000 clusters
 constexpr size_t kImageBytes = 4u << 20;
 constexpr size_t kOrderBytes = kNoallocScratchBytes - kCtrlBytes - kImageBytes;
 constexpr int64_t kNoallocMaxTraj = (int64_t)(kOrderBytes / sizeof(int32_t));

@@ -328,7 +328,7 @@ cosims_status cosims_probe_peaks(int32_t device, double *fp32_tflops, double *fp
  * queue, work order and counters live in one static 12 MiB device array that
  * every GPU loading this library holds until the process exits.  Limits: at
  * most 2,096,128 trajectories per call and molecule images of at most 4 MiB
- * (about 100 bytes per atom and at most 820 per cluster: every molecule within
+ * (about 100 bytes per atom and at most 850 per cluster: every molecule within
  * the 16384-atom limit fits with up to 3000 clusters); larger requests return
  * COSIMS_ERR_UNSUPPORTED before any device work.  The first call on a device
  * looks up its array (cudaGetSymbolAddress, with that device current; the
