@@ -728,6 +728,22 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
           }
         }
         const int nmax = na > nb ? na : nb;
+        if (TYPE == 1 && !es) {
+          // variant 1's LJ-only clusters are far ones inside the dispersion
+          // radius: every atom takes the cluster's band parameters, so the
+          // per-atom LJ records are not read.  The prefactor is the cluster's
+          // for its atoms (the first n_atoms slots of its blocks) and 0 for
+          // padding, as the records' atom flag gives it.
+          const float2 sig = f2(CA.qsig6, CB.qsig6);
+          const int ra = CA.n_atoms, rb = has_b ? CB.n_atoms : 0;
+          for (int k = sub; k < nmax; k += split) {
+            const int ka = k < na ? CA.a0 + k : inert0 + (k & (kClusterBlock - 1));
+            const int kb = k < nb ? CB.a0 + k : inert0 + (k & (kClusterBlock - 1));
+            const float2 eps = f2(k < ra ? CA.qeps : 0.0f, k < rb ? CB.qeps : 0.0f);
+            pair2<TYPE>(m.a4[ka], m.a4[kb], sig, eps, false, hx2, hy2, hz2, lx2, ly2, lz2, t);
+          }
+          continue;
+        }
         for (int k = sub; k < nmax; k += split) {
           const int ka = k < na ? CA.a0 + k : inert0 + (k & (kClusterBlock - 1));
           const int kb = k < nb ? CB.a0 + k : inert0 + (k & (kClusterBlock - 1));
