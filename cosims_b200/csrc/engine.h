@@ -64,7 +64,7 @@ __host__ __device__ constexpr bool blocked_layout(int force_type) {
 constexpr float kPadCoord = 1.0e6f;                // pad atoms sit this far out (Angstrom)
 constexpr int kMixedMaxBlock = 768;                // threads per CTA of the mixed kernels (80 registers)
 constexpr int kMixedFarBlock = 640;                // variants 1, 2: 96 registers, 20 warps a CTA
-constexpr int kBatchMaxBlock = 512;                // threads per CTA of the batched kernel
+constexpr int kBatchMaxBlock = 640;                // threads per CTA of the batched kernel (96 registers)
 constexpr int kTrajStateBytes = 200;               // one trajectory's integrator state
 constexpr int kGroupStateBytes = 240;              // TrajState + a group's counters (shared memory)
 constexpr int kWideSlotFloats = 24;                // per-warp reduction slot of a wide group
