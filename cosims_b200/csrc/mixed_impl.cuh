@@ -301,14 +301,11 @@ struct Far2 {
 
 __device__ __forceinline__ float2 neg2(const float2 &a) { return f2(-a.x, -a.y); }
 // far_terms for two clusters at once, one per half of the packed
-// instructions, from their distances (the FP64 differences rounded to FP32,
-// as in far_terms).  Replaced clusters carry a zero dipole in the F32 image;
-// the null cluster (index n_clusters, zero moments) adds exactly 0 at any
-// finite distance, so it fills a half that has no far cluster.
-//
-// far2_core takes the two clusters' separations, their squares, r2 and 1/r,
-// charges, dipoles and (order 2) quadrupoles.  Every term carries a power of
-// 1/r, so a half whose 1/r is 0 adds exactly 0 (with finite separations).
+// instructions (forceAccel.cpp:258-337), from the two clusters' separations,
+// their squares, r2 and 1/r, charges, dipoles and (order 2) quadrupoles.
+// Replaced clusters carry a zero dipole.  Every term carries a power of 1/r,
+// so a half whose 1/r is 0 adds exactly 0 (with finite separations), and a
+// null entry (zero moments) adds exactly 0 at any finite distance.
 __device__ __forceinline__ void far2_core(int order, const float2 &dx, const float2 &dy,
                                           const float2 &dz, const float2 &xx, const float2 &yy,
                                           const float2 &zz, const float2 &r2, const float2 &r_1,
@@ -378,17 +375,6 @@ __device__ __forceinline__ void far2_core(int order, const float2 &dx, const flo
     s.Maxz = __ffma2_rn(p5, __ffma2_rn(t2, dx, __fmul2_rn(neg2(t0), dz)), s.Maxz);
     s.Mayz = __ffma2_rn(p5, __ffma2_rn(t2, dy, __fmul2_rn(neg2(t1), dz)), s.Mayz);
   }
-}
-
-__device__ __forceinline__ void far2(const View &m, int ia, int ib, int order, const float2 &dx,
-                                     const float2 &dy, const float2 &dz, Far2 &s) {
-  const ClusterF32 &A = m.cl[ia];
-  const ClusterF32 &B = m.cl[ib];
-  const float2 xx = __fmul2_rn(dx, dx), yy = __fmul2_rn(dy, dy), zz = __fmul2_rn(dz, dz);
-  const float2 r2 = __fadd2_rn(__fadd2_rn(xx, yy), zz);
-  const float2 r_1 = f2(rsqrt_ftz(r2.x), rsqrt_ftz(r2.y));
-  far2_core(order, dx, dy, dz, xx, yy, zz, r2, r_1, f2(A.q, B.q), f2(A.dip[0], B.dip[0]),
-            f2(A.dip[1], B.dip[1]), f2(A.dip[2], B.dip[2]), A.quad, B.quad, s);
 }
 
 // The 12 far-field sums of a lane (both halves added), in the order of the
@@ -560,12 +546,10 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
     int n_es = 0, n_lj = 0;
     // the far-table pass leaves the pair counts of the listed clusters to pass 2
     bool count_listed = false;
-    // one round: the clusters c0 + lane; returns whether the lane's cluster
-    // is far, with its distance rounded to FP32
-    auto classify = [&](int c0, float &fx, float &fy, float &fz) {
+    // one round: the clusters c0 + lane (FP64 tests, list entries, counters)
+    auto classify = [&](int c0) {
       const int c = c0 + lane;
       uint32_t mode = 0;
-      bool far = false;
       if (c < m.nc) {
         const ClusterF32 &C = m.cl[c];
         const double d0 = pos[0] - C.cx, d1 = pos[1] - C.cy, d2 = pos[2] - C.cz;
@@ -575,7 +559,6 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
           mode = in_disp ? M_LJ : 0;
         } else if (r2 > C.mpr2) {
           w.far++;
-          far = true;
           mode = TYPE == 2 ? M_LJ : (in_disp ? M_LJQ : 0);
         } else {
           mode = M_ES | ((TYPE == 2 || in_disp) ? M_LJ : 0);
@@ -584,7 +567,6 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
         if (mode & M_ES) w.es += cnt;
         else if (mode) w.lj += cnt;
         if ((mode & M_ES) && !(mode & M_LJ)) w.nl += cnt;
-        fx = (float)d0; fy = (float)d1; fz = (float)d2;
       }
       const bool es = (mode & M_ES) != 0, ljo = mode != 0 && !es;
       const unsigned m_es = (__ballot_sync(0xffffffffu, es) >> gbase) & gbits;
@@ -594,7 +576,6 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
       if (ljo) list[m.nc - 1 - n_lj - __popc(m_lj & below)] = e;
       n_es += __popc(m_es);
       n_lj += __popc(m_lj);
-      return far;
     };
     if (Traits<TYPE>::kFar && PACKED_FAR && G >= 16) {
       // far field in the same pass (variants 1 and 2, G >= 16), from the
@@ -685,10 +666,7 @@ __device__ __forceinline__ void force(const View &m, const DevParams &p, const d
       far_share = reduce_scatter<12>(fv, G, lane, idx);
       far_reduced = true;
     } else {
-      for (int c0 = 0; c0 < m.nc; c0 += G) {
-        float x, y, z;
-        classify(c0, x, y, z);
-      }
+      for (int c0 = 0; c0 < m.nc; c0 += G) classify(c0);
     }
     ln.sync();
     // pass 2: the listed clusters, two at a time per (half-)group in the two
