@@ -179,7 +179,7 @@ cosims_status cosims_ctx_create(const cosims_molecule *mol, const cosims_params 
 void cosims_ctx_destroy(cosims_ctx *ctx);
 
 /* Launch shape: lanes per trajectory (1,2,4,...,32; the plain form accepts 1
- * only) and threads per CTA (plain: up to 128; mixed: up to 768, or 512 for
+ * only) and threads per CTA (plain: up to 128; mixed: up to 768, or 640 for
  * force variants 1 and 2; by default chosen per run for the most resident
  * threads).  0 keeps the current choice.
  * get_launch reports the CTA size of the last run when it was chosen. */
