@@ -387,7 +387,7 @@ int mode_stride_for(const MolImage &img, int force_type) {
 
 // Launch shape: threads per CTA, CTAs, dynamic shared memory, whether the
 // image is staged, and the per-group mode scratch.  block_threads 0 (mixed
-// form) picks the CTA size (256, 512 or 768 threads, at most 512 for the
+// form) picks the CTA size (256, 512 or 768 threads; 256, 512 or 640 for the
 // far-field variants 1 and 2: the occupancy query refuses more) that keeps the
 // most threads resident per SM, preferring a staged image: one staged copy of
 // the molecule serves every group of a CTA.

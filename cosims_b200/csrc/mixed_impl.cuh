@@ -471,7 +471,7 @@ struct NarrowLanes {
 // taken per cluster in pass 1 (or per evaluation), not per pair.
 // PACKED_FAR: the far field of variants 1 and 2 in packed instructions, for
 // kernels with the registers for it (the single-molecule kernel of those
-// variants and the batched kernel run 512-thread CTAs at 128 registers).
+// variants and the batched kernel run 640-thread CTAs at 96 registers).
 template <int TYPE, bool PACKED_FAR, class L>
 __device__ __forceinline__ void force(const View &m, const DevParams &p, const double pos[3],
                                       double acc[3], L &ln, uint8_t *modes, WorkM &w) {
@@ -1698,9 +1698,10 @@ __device__ __noinline__ void wide_phase(unsigned char *smem, uint32_t img_bytes,
 
 // Threads per CTA at most: 768 gives 80 registers a thread, enough for the
 // wide groups' register-resident state (the narrow phase runs as fast at 24
-// warps per SM as at 32).  The far-field variants 1 and 2 take 512 threads
-// and 128 registers: their packed far-field pass holds 12 packed sums and
-// the multipole temporaries, which spill at 80.
+// warps per SM as at 32).  The far-field variants 1 and 2 take 640 threads
+// and 96 registers: their packed far-field pass holds 12 packed sums and
+// the multipole temporaries, which spill about 200 bytes a thread at 80
+// (at 96 a few dozen; 640 threads measured faster than 512 at 128).
 template <int TYPE>
 struct KernelShape {
   static constexpr int kMaxThreads = (TYPE == 1 || TYPE == 2) ? kMixedFarBlock : kMixedMaxBlock;

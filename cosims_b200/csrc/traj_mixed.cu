@@ -30,7 +30,7 @@ struct BatchSource {
   int mol;                    // the staged molecule
   long long base;             // its first slot in the batch arrays
 };
-// 512-thread CTAs at 128 registers: room for the packed far-field pass
+// 640-thread CTAs at 96 registers: room for the packed far-field pass
 template <> struct PackedFar<BatchSource> { static constexpr bool value = true; };
 __device__ __forceinline__ cosims_traj_out *out_of(const BatchSource &s) { return s.a->out; }
 __device__ __forceinline__ long long budget_of(const BatchSource &) { return 0; }
